@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""KSG pairs/s on B200 for the reference-size workload: 247 atoms x 2000 frames,
+k = 100, float32-rounded synthetic positions (16 latent AR(1) modes, loadings
+0.08 nm), the reference's CPU path timed beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one full KSG MI matrix (all 30,381 pairs: normalisation,
+neighbour statistics, ordered MI reduction) over coordinates already resident
+in HBM; the L2 is flushed (a 256 MiB write) between timed steps.  `value` is
+whole-job pairs/s; `e2e` is the same metric through the public C-ABI call
+gc_ksg_matrix from pinned host memory (H2D of the coordinates and D2H of the
+pair MI inside the timed region).  With N > 1 (torchrun, one rank per GPU)
+every rank processes its own independent trajectory (weak scaling, no
+data-path collective); timing is max over ranks.
+
+--impl reference times the reference's own OpenMP CPU implementation
+(oracle/_ref, the unmodified lib/*.cpp compiled here) on a bounded random
+sample of pairs of the same workload per step, with every host thread.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "KSG pairs/s at 247 atoms×2000 fr k=100; plain vs MLP-screened at |Δr|≤1e-2"
+UNIT = "pairs/s"
+WORKLOAD = "KSG r(MI) matrix, 247 atoms x 2000 frames, k=100, float32-rounded synthetic positions"
+FP32_OPS_PER_EVAL = 12  # 6 |d|, 5 max, 1 threshold compare per joint distance-eval
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: str):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", self.gpu], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, flag in zip(names, parts[5:9]):
+                if flag.lower() in ("active", "1", "yes"):
+                    reasons.add(nm)
+        self.path.unlink(missing_ok=True)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def traffic_from_profiles(kernel: str):
+    """DRAM bytes per launch recorded from an ncu capture (profiles/*.txt)."""
+    for f in sorted((ROOT / "profiles").glob("*.txt")):
+        for line in f.read_text().splitlines():
+            if line.startswith(f"traffic_bytes_per_launch[{kernel}]"):
+                try:
+                    return float(line.split("=", 1)[1].split()[0])
+                except (IndexError, ValueError):
+                    return None
+    return None
+
+
+def cpu_baseline_sample(x, k, seconds: float, seed: int = 7):
+    """Reference OpenMP KSG (kraskov_prepare + kraskov_wrap, dynamic,1) on a
+    random pair sample sized to about `seconds` of work on all host threads."""
+    from oracle import Reference
+    ref = Reference()
+    n = x.shape[0]
+    rng = np.random.default_rng(seed)
+    threads = os.cpu_count() or 1
+
+    def sample(m):
+        a1 = rng.integers(1, n, size=m)
+        a2 = np.array([rng.integers(0, a) for a in a1])
+        t0 = time.perf_counter()
+        ref.ksg_pairs(x, k, a1, a2, nthreads=threads)
+        return time.perf_counter() - t0
+
+    m0 = max(threads, 8)
+    dt = sample(m0)
+    m = int(max(m0, min(4096, m0 * seconds / max(dt, 1e-3))))
+    dt = sample(m)
+    return {"value": m / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{m} random pairs of the 247x2000 k=100 matrix through the reference's "
+                      f"kraskov_prepare+kraskov_wrap OpenMP loop ({dt:.1f} s)"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from gmx_correlation_b200.synth import config_traj
+    try:
+        from oracle import Reference
+        ref = Reference()
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU library not built: {e}"}))
+        return 0
+    x = config_traj("ref")
+    k, n = 100, x.shape[0]
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(11)
+    # size one step to ~8 s of CPU work
+    a1 = rng.integers(1, n, size=threads * 2)
+    a2 = np.array([rng.integers(0, a) for a in a1])
+    t0 = time.perf_counter()
+    ref.ksg_pairs(x, k, a1, a2, nthreads=threads)
+    rate = len(a1) / (time.perf_counter() - t0)
+    per_step = int(max(threads, min(4096, rate * 8.0)))
+    times = []
+    for s in range(args.warmup + args.steps):
+        a1 = rng.integers(1, n, size=per_step)
+        a2 = np.array([rng.integers(0, a) for a in a1])
+        t0 = time.perf_counter()
+        ref.ksg_pairs(x, k, a1, a2, nthreads=threads)
+        if s >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    value = per_step / (ms / 1e3)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "pairs_per_step": per_step, "variant": "plain",
+                   "sample": "random pairs of the 30,381-pair matrix, new sample each step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{per_step} random pairs per step through kraskov_prepare+kraskov_wrap "
+                                   f"(OpenMP dynamic,1, {threads} threads)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    import gmx_correlation_b200 as gc
+    from gmx_correlation_b200.synth import CONFIGS, synth_traj
+
+    ws, rank, local = dist_env()
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    else:
+        torch.cuda.set_device(local)
+    c = CONFIGS["ref"]
+    x = synth_traj(c["natoms"], c["nframes"], c["n_modes"], c["sigma_l"], seed=c["seed"] + rank, fp32=c["fp32"])
+    n, T, k = x.shape[0], x.shape[1], c["k"]
+    npairs = n * (n - 1) // 2
+    dev = torch.device("cuda", local)
+    d_xyz = torch.from_numpy(x).to(dev)
+    d_out = torch.empty(npairs, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    plan = gc.KsgPlan(n, T, k, device=local)
+    stream = torch.cuda.current_stream(dev)
+
+    for _ in range(args.warmup):
+        plan.run(d_xyz.data_ptr(), d_out.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        plan.sync()
+
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    gpu_index = vis.split(",")[local] if vis else str(local)
+    sampler = ClockSampler(gpu_index)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    sampler.start()
+    step_ms, kern_ms = [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.run(d_xyz.data_ptr(), d_out.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        step_ms.append(e0.elapsed_time(e1))
+        kern_ms.append(plan.kernel_ms)
+    torch.cuda.synchronize(dev)
+    if pg:
+        pg.barrier()
+    clocks = sampler.stop()
+    plan.sync()
+    total_ms = sum(step_ms)
+    launches = plan.launches * args.steps
+    if pg:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = ws * npairs / (ms_per_step / 1e3)
+
+    # end to end through the public C-ABI call, pinned host input
+    x_pinned = torch.from_numpy(x).pin_memory().numpy()
+    gc.kraskov_corrmatrix(x_pinned, k, device=local)
+    e2e_steps = max(1, min(args.steps, 3))
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        gc.kraskov_corrmatrix(x_pinned, k, device=local)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if pg:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    if rank == 0:
+        mix_ops, fma_flops = gc.probe_fp32(local)
+        kms = statistics.mean(kern_ms)
+        evals = npairs * T * (T - 1)
+        achieved = evals * FP32_OPS_PER_EVAL / (kms / 1e3)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "variant": "plain", "pairs_per_gpu": npairs,
+                       "l2": "256 MiB flush between timed steps", "path": "exact-fp64 brute force"},
+            "e2e": {"value": ws * npairs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(x.nbytes),
+                    "d2h_bytes_per_step": int(npairs * 8)},
+            "gpu_launches": launches,
+            "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": mix_ops / 1e12, "unit": "TOP/s",
+                         "frac": achieved / mix_ops, "traffic": traffic_from_profiles("ksg_exact_kernel"),
+                         "kernel": "ksg_exact_kernel", "kernel_ms": kms,
+                         "distance_evals_per_s": evals / (kms / 1e3),
+                         "peak_note": "measured FADD+FMNMX lane-op rate of this GPU (gc_probe_fp32); "
+                                      f"FFMA {fma_flops / 1e12:.1f} TFLOP/s"},
+            "clocks": clocks,
+        }
+        if ws == 1 and not args.no_cpu_baseline:
+            try:
+                out["cpu_baseline"] = cpu_baseline_sample(x, k, args.cpu_seconds)
+            except Exception as e:  # noqa: BLE001
+                out["cpu_baseline"] = {"unavailable": str(e)}
+        print(json.dumps(out))
+    plan.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    args.warmup = max(args.warmup, 3)  # timing rule: at least three untimed warm-up steps
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,304 @@
+"""gmx_correlation_b200 -- all-pairs generalized correlation on NVIDIA B200.
+
+Python host binding of the C ABI in include/gmx_corr_b200.h.  The function
+names and argument meanings follow the reference's estimator interface
+(scdantu/gmx_correlation lib/correlation_core.h, lib/gcmi.h,
+lib/transfer_entropy.h):
+
+    kraskov_corrmatrix(x, k)      KSG (Kraskov alg. 2) MI matrix
+    gauss_corrmatrix(x)           Gaussian (-linear) MI matrix
+    gcmi_corrmatrix(x)            Gaussian-copula MI matrix
+    te_matrix(x, k, lag)          transfer entropy, te[a1, a2] = TE(a2 -> a1)
+    pearsify(mat, dim)            r(MI) = sqrt(1 - exp(-2 MI / dim))
+    write_matrix / write_xpm_matrix / read_matrix
+
+``x`` is the mean-centred t_traj block, shape (natoms, nframes, 3) float64.
+Every estimator computes on the GPU; if the CUDA library is missing or no
+device is present the call raises -- there is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+__all__ = [
+    "GCError", "lib", "gpu_available", "kraskov_corrmatrix", "gauss_corrmatrix",
+    "gcmi_corrmatrix", "te_matrix", "kraskov_prepare", "kraskov_wrap", "pearsify",
+    "write_matrix", "write_xpm_matrix", "read_matrix", "KsgPlan", "PATH_AUTO",
+    "PATH_EXACT_FP64", "LIB_PATH", "probe_fp32",
+]
+
+LIB_PATH = Path(__file__).resolve().parent / "libgmxcorr_b200.so"
+PATH_AUTO = 0
+PATH_EXACT_FP64 = 1
+
+_STATUS = {
+    1: "invalid argument", 2: "no CUDA device", 3: "CUDA error", 4: "zero-variance component",
+    5: "non-finite coordinate", 6: "out of device memory", 7: "I/O error", 8: "internal error",
+    9: "device wait timed out",
+}
+
+
+class GCError(RuntimeError):
+    """A C-ABI call failed; ``status`` holds the gc_status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{_STATUS.get(status, status)}] {message}")
+        self.status = status
+
+
+class _TrajView(ctypes.Structure):
+    _fields_ = [("natoms", ctypes.c_int), ("nframes", ctypes.c_int),
+                ("xyz", ctypes.POINTER(ctypes.c_double)),
+                ("rows", ctypes.POINTER(ctypes.POINTER(ctypes.c_double)))]
+
+
+class _Opts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("path", ctypes.c_int), ("pair_begin", ctypes.c_long),
+                ("pair_end", ctypes.c_long), ("stream", ctypes.c_void_p),
+                ("detail_nx", ctypes.POINTER(ctypes.c_int32)),
+                ("detail_ny", ctypes.POINTER(ctypes.c_int32))]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded libgmxcorr_b200.so (raises if it was never built)."""
+    global _lib
+    if _lib is None:
+        path = Path(os.environ.get("GMXCORR_B200_LIB", LIB_PATH))
+        if not path.exists():
+            raise GCError(3, f"{path} is missing: build it with `python -m gmx_correlation_b200.build`")
+        L = ctypes.CDLL(str(path))
+        dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)
+        L.gc_last_error.restype = ctypes.c_char_p
+        L.gc_opts_init.argtypes = [ctypes.POINTER(_Opts)]
+        L.gc_ksg_matrix.argtypes = [ctypes.POINTER(_TrajView), ctypes.c_int, ctypes.POINTER(_Opts), dp]
+        L.gc_gauss_matrix.argtypes = [ctypes.POINTER(_TrajView), ctypes.POINTER(_Opts), dp]
+        L.gc_gcmi_matrix.argtypes = [ctypes.POINTER(_TrajView), ctypes.POINTER(_Opts), dp]
+        L.gc_te_matrix.argtypes = [ctypes.POINTER(_TrajView), ctypes.c_int, ctypes.c_int,
+                                   ctypes.POINTER(_Opts), dp]
+        L.gc_ksg_prepare.argtypes = [ctypes.POINTER(_TrajView), ctypes.POINTER(_Opts), dp, dp, dp]
+        L.gc_ksg_pair.argtypes = [dp, ctypes.c_int, ctypes.c_int, dp, ctypes.POINTER(_Opts), dp]
+        L.gc_pearsify.argtypes = [dp, ctypes.c_int, ctypes.c_int]
+        L.gc_pearsify.restype = None
+        L.gc_write_matrix.argtypes = [dp, ctypes.c_int, ctypes.c_char_p]
+        L.gc_write_xpm.argtypes = [dp, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p]
+        L.gc_ksg_plan_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Opts),
+                                         ctypes.POINTER(ctypes.c_void_p)]
+        L.gc_ksg_plan_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.gc_ksg_plan_sync.argtypes = [ctypes.c_void_p]
+        L.gc_ksg_plan_pairs.argtypes = [ctypes.c_void_p]
+        L.gc_ksg_plan_pairs.restype = ctypes.c_long
+        L.gc_ksg_plan_launches.argtypes = [ctypes.c_void_p]
+        L.gc_ksg_plan_kernel_ms.argtypes = [ctypes.c_void_p]
+        L.gc_ksg_plan_kernel_ms.restype = ctypes.c_float
+        L.gc_probe_fp32.argtypes = [ctypes.c_int, dp, dp]
+        L.gc_ksg_plan_destroy.argtypes = [ctypes.c_void_p]
+        L.gc_ksg_plan_destroy.restype = None
+        _ = ip
+        _lib = L
+    return _lib
+
+
+def _check(status: int):
+    if status != 0:
+        raise GCError(status, lib().gc_last_error().decode(errors="replace"))
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _coords(x) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    if x.ndim != 3 or x.shape[2] != 3:
+        raise ValueError("coordinates must have shape (natoms, nframes, 3)")
+    return x
+
+
+def _view(x: np.ndarray) -> _TrajView:
+    v = _TrajView()
+    v.natoms, v.nframes = x.shape[0], x.shape[1]
+    v.xyz = _dptr(x)
+    v.rows = None
+    return v
+
+
+def _opts(device=-1, path=PATH_AUTO, pairs=None, stream=None) -> _Opts:
+    o = _Opts()
+    lib().gc_opts_init(ctypes.byref(o))
+    o.device, o.path = device, path
+    if pairs is not None:
+        o.pair_begin, o.pair_end = int(pairs[0]), int(pairs[1])
+    if stream is not None:
+        o.stream = ctypes.c_void_p(stream)
+    return o
+
+
+def probe_fp32(device: int = -1):
+    """(FADD+FMNMX lane-ops/s, FFMA flop/s) measured on the device."""
+    mix, fma = ctypes.c_double(), ctypes.c_double()
+    _check(lib().gc_probe_fp32(device, ctypes.byref(mix), ctypes.byref(fma)))
+    return mix.value, fma.value
+
+
+def gpu_available() -> bool:
+    """True when a compute-capability 10.x (B200) device is visible."""
+    return bool(lib().gc_gpu_available())
+
+
+def kraskov_corrmatrix(x, k: int, *, path: int = PATH_AUTO, device: int = -1, pairs=None,
+                       detail: bool = False):
+    """KSG MI matrix (natoms x natoms), diagonal 2000, as kraskov_corrmatrix.
+
+    ``pairs=(begin, end)`` computes only that shard of the pair list
+    p = a1*(a1-1)/2 + a2.  With ``detail=True`` also returns the per-query
+    counts (nx, ny), each of shape (npairs_in_shard, nframes).
+    """
+    x = _coords(x)
+    n, T = x.shape[0], x.shape[1]
+    out = np.zeros(n * n)
+    o = _opts(device, path, pairs)
+    nx = ny = None
+    if detail:
+        npairs = n * (n - 1) // 2
+        b, e = (0, npairs) if pairs is None else (pairs[0], pairs[1] if pairs[1] > 0 else npairs)
+        nx = np.zeros((max(e - b, 0), T), np.int32)
+        ny = np.zeros_like(nx)
+        o.detail_nx = nx.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        o.detail_ny = ny.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    v = _view(x)
+    _check(lib().gc_ksg_matrix(ctypes.byref(v), int(k), ctypes.byref(o), _dptr(out)))
+    mat = out.reshape(n, n)
+    return (mat, nx, ny) if detail else mat
+
+
+def gauss_corrmatrix(x, *, device: int = -1) -> np.ndarray:
+    x = _coords(x)
+    n = x.shape[0]
+    out = np.zeros(n * n)
+    v, o = _view(x), _opts(device)
+    _check(lib().gc_gauss_matrix(ctypes.byref(v), ctypes.byref(o), _dptr(out)))
+    return out.reshape(n, n)
+
+
+def gcmi_corrmatrix(x, *, device: int = -1) -> np.ndarray:
+    x = _coords(x)
+    n = x.shape[0]
+    out = np.zeros(n * n)
+    v, o = _view(x), _opts(device)
+    _check(lib().gc_gcmi_matrix(ctypes.byref(v), ctypes.byref(o), _dptr(out)))
+    return out.reshape(n, n)
+
+
+def te_matrix(x, k: int, lag: int = 1, *, path: int = PATH_AUTO, device: int = -1) -> np.ndarray:
+    """te[a1, a2] = TE(a2 -> a1, lag); zero diagonal; zeros if nframes - lag <= k."""
+    x = _coords(x)
+    n = x.shape[0]
+    out = np.zeros(n * n)
+    v, o = _view(x), _opts(device, path)
+    _check(lib().gc_te_matrix(ctypes.byref(v), int(k), int(lag), ctypes.byref(o), _dptr(out)))
+    return out.reshape(n, n)
+
+
+def kraskov_prepare(x, *, device: int = -1):
+    """(X [3n, T], psi [T+1], scal [3n]) exactly as kraskov_prepare builds them."""
+    x = _coords(x)
+    n, T = x.shape[0], x.shape[1]
+    X = np.zeros((3 * n, T))
+    psi = np.zeros(T + 1)
+    scal = np.zeros(3 * n)
+    v, o = _view(x), _opts(device)
+    _check(lib().gc_ksg_prepare(ctypes.byref(v), ctypes.byref(o), _dptr(X), _dptr(psi), _dptr(scal)))
+    return X, psi, scal
+
+
+def kraskov_wrap(X, psi, a1: int, a2: int, k: int, *, device: int = -1) -> float:
+    """MI of one pair from prepared rows, as kraskov_wrap (a1's rows first)."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    T = X.shape[1]
+    rows = np.ascontiguousarray(np.concatenate([X[3 * a1:3 * a1 + 3], X[3 * a2:3 * a2 + 3]]))
+    psi = np.ascontiguousarray(psi, dtype=np.float64)
+    mi = ctypes.c_double()
+    o = _opts(device)
+    _check(lib().gc_ksg_pair(_dptr(rows), T, int(k), _dptr(psi), ctypes.byref(o), ctypes.byref(mi)))
+    return mi.value
+
+
+def pearsify(mat: np.ndarray, dim: int = 3) -> np.ndarray:
+    """In-place r(MI) conversion (returns ``mat``)."""
+    if not (isinstance(mat, np.ndarray) and mat.dtype == np.float64 and mat.flags.c_contiguous):
+        raise ValueError("pearsify needs a C-contiguous float64 array")
+    lib().gc_pearsify(_dptr(mat), int(mat.shape[0]), int(dim))
+    return mat
+
+
+def write_matrix(mat: np.ndarray, path) -> None:
+    m = np.ascontiguousarray(mat, dtype=np.float64)
+    _check(lib().gc_write_matrix(_dptr(m), m.shape[0], str(path).encode()))
+
+
+def write_xpm_matrix(mat: np.ndarray, path, title: str = "", legend: str = "") -> None:
+    m = np.ascontiguousarray(mat, dtype=np.float64)
+    _check(lib().gc_write_xpm(_dptr(m), m.shape[0], str(path).encode(), title.encode(), legend.encode()))
+
+
+def read_matrix(path) -> np.ndarray:
+    """Parse a correl.dat file (the consumer's reading of the format:
+    optional `N x M [ ... ]` wrapper, values written column-major)."""
+    raw = Path(path).read_text()
+    inner = raw[raw.index("[") + 1: raw.rindex("]")] if "[" in raw else raw
+    vals = [float(v) for v in inner.split() if v not in ("{", "}")]
+    n = int(round(len(vals) ** 0.5))
+    if n * n != len(vals):
+        raise ValueError(f"{len(vals)} values do not form a square matrix")
+    return np.array(vals).reshape(n, n).T
+
+
+class KsgPlan:
+    """Device-resident KSG plan: inputs already in HBM, nothing allocated per run."""
+
+    def __init__(self, natoms: int, nframes: int, k: int, *, device: int = -1, pairs=None,
+                 path: int = PATH_AUTO):
+        self._h = ctypes.c_void_p()
+        o = _opts(device, path, pairs)
+        _check(lib().gc_ksg_plan_create(natoms, nframes, k, ctypes.byref(o), ctypes.byref(self._h)))
+        self.natoms, self.nframes, self.k = natoms, nframes, k
+
+    @property
+    def pairs(self) -> int:
+        return int(lib().gc_ksg_plan_pairs(self._h))
+
+    @property
+    def launches(self) -> int:
+        return int(lib().gc_ksg_plan_launches(self._h))
+
+    def run(self, d_xyz: int, d_pair_mi: int, stream: int | None = None) -> None:
+        """Enqueue one full KSG pass; pointers are raw device addresses."""
+        _check(lib().gc_ksg_plan_run(self._h, ctypes.c_void_p(d_xyz), ctypes.c_void_p(d_pair_mi),
+                                     ctypes.c_void_p(stream or 0)))
+
+    def sync(self) -> None:
+        _check(lib().gc_ksg_plan_sync(self._h))
+
+    @property
+    def kernel_ms(self) -> float:
+        """Device time of the neighbour kernel(s) of the last completed run."""
+        return float(lib().gc_ksg_plan_kernel_ms(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            lib().gc_ksg_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

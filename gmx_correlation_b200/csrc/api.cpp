@@ -1,0 +1,633 @@
+// C ABI of gmx_correlation_b200 (declared in include/gmx_corr_b200.h).
+//
+// Host side of the all-pairs path: argument checks with the reference's
+// messages, device selection, workspace plans, host<->device staging and
+// matrix assembly.  Every estimator computes on the GPU; there is no CPU
+// fallback (a missing device is an error).
+
+#include "gmx_corr_b200.h"
+#include "gc_internal.h"
+#include "gc_geom.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_last_error;
+
+gc_status fail(gc_status st, const std::string& msg)
+{
+    g_last_error = msg;
+    return st;
+}
+
+#define GC_TRY_CUDA(call)                                                                            \
+    do                                                                                               \
+    {                                                                                                \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess)                                                                       \
+            return fail(e_ == cudaErrorMemoryAllocation ? GC_ERR_OUT_OF_MEMORY : GC_ERR_CUDA,         \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+    } while (0)
+
+#define GC_TRY(expr)                                                                                 \
+    do                                                                                               \
+    {                                                                                                \
+        gc_status s_ = (expr);                                                                       \
+        if (s_ != GC_OK)                                                                             \
+            return s_;                                                                               \
+    } while (0)
+
+// Switches to the requested device for the lifetime of the guard.
+struct DeviceScope
+{
+    int       prev = -1;
+    gc_status st   = GC_OK;
+    explicit DeviceScope(int dev)
+    {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+        {
+            cudaGetLastError();
+            st = fail(GC_ERR_NO_DEVICE, "no CUDA device available (this build has no CPU path)");
+            return;
+        }
+        cudaGetDevice(&prev);
+        if (dev >= 0)
+        {
+            if (dev >= n)
+            {
+                st = fail(GC_ERR_INVALID, "device ordinal out of range");
+                return;
+            }
+            if (cudaSetDevice(dev) != cudaSuccess)
+                st = fail(GC_ERR_CUDA, "cudaSetDevice failed");
+        }
+    }
+    ~DeviceScope()
+    {
+        if (prev >= 0)
+            cudaSetDevice(prev);
+    }
+};
+
+template <class T>
+struct DevBuf
+{
+    T*     p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { reset(); }
+    void reset()
+    {
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    gc_status alloc(size_t count)
+    {
+        reset();
+        if (count == 0)
+            count = 1;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess)
+        {
+            cudaGetLastError();
+            p = nullptr;
+            return fail(e == cudaErrorMemoryAllocation ? GC_ERR_OUT_OF_MEMORY : GC_ERR_CUDA,
+                        std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        n = count;
+        return GC_OK;
+    }
+};
+
+gc_opts defaults()
+{
+    gc_opts o;
+    gc_opts_init(&o);
+    return o;
+}
+
+// digamma table of kraskov_prepare (lib/kraskov.cpp:2217-2219) and
+// digamma_table (lib/transfer_entropy.cpp:41-48): psi[0] = 0,
+// psi[1] = -0.57721566490153, psi[n+1] = psi[n] + 1/n.
+std::vector<double> digamma_table(int N)
+{
+    std::vector<double> psi((size_t)N + 1, 0.0);
+    if (N >= 1)
+        psi[1] = -0.57721566490153;
+    for (int n = 1; n < N; ++n)
+        psi[n + 1] = psi[n] + 1 / (1.0 * n);
+    return psi;
+}
+
+gc_status check_view(const gc_traj_view* v)
+{
+    if (!v)
+        return fail(GC_ERR_INVALID, "null trajectory view");
+    if ((v->xyz == nullptr) == (v->rows == nullptr))
+        return fail(GC_ERR_INVALID, "trajectory view needs exactly one of xyz / rows");
+    if (v->natoms < 0 || v->nframes < 0)
+        return fail(GC_ERR_INVALID, "negative trajectory size");
+    if (v->rows)
+        for (int a = 0; a < v->natoms; ++a)
+            if (!v->rows[a])
+                return fail(GC_ERR_INVALID, "null atom row in trajectory view");
+    return GC_OK;
+}
+
+// Uploads the view's coordinates into a contiguous device block.
+gc_status upload_traj(const gc_traj_view* v, double* d_xyz, cudaStream_t s)
+{
+    const size_t row = (size_t)v->nframes * 3;
+    if (v->xyz)
+    {
+        GC_TRY_CUDA(cudaMemcpyAsync(d_xyz, v->xyz, sizeof(double) * row * v->natoms, cudaMemcpyHostToDevice, s));
+    }
+    else
+    {
+        for (int a = 0; a < v->natoms; ++a)
+            GC_TRY_CUDA(cudaMemcpyAsync(d_xyz + row * a, v->rows[a], sizeof(double) * row, cudaMemcpyHostToDevice, s));
+    }
+    return GC_OK;
+}
+
+gc_status status_to_error(int st)
+{
+    if (st & gc::kStatNonFinite)
+        return fail(GC_ERR_NONFINITE, "non-finite coordinate in the trajectory");
+    if (st & gc::kStatZeroVariance)
+        return fail(GC_ERR_ZERO_VARIANCE,
+                    "a coordinate component has zero variance over the frames (the reference divides by it)");
+    if (st & gc::kStatTimeout)
+        return fail(GC_ERR_TIMEOUT, "a bounded device wait ran out");
+    if (st & gc::kStatInternal)
+        return fail(GC_ERR_INTERNAL, "device-side consistency check failed");
+    return GC_OK;
+}
+
+struct StreamScope
+{
+    cudaStream_t s     = nullptr;
+    bool         owned = false;
+    gc_status    init(void* user)
+    {
+        if (user)
+        {
+            s = (cudaStream_t)user;
+            return GC_OK;
+        }
+        GC_TRY_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        owned = true;
+        return GC_OK;
+    }
+    ~StreamScope()
+    {
+        if (owned && s)
+            cudaStreamDestroy(s);
+    }
+};
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// KSG plan
+// ---------------------------------------------------------------------------
+
+struct gc_ksg_plan
+{
+    int          device = 0;
+    int          natoms = 0, T = 0, K = 0, path = GC_PATH_AUTO;
+    long         pair_begin = 0, pair_count = 0;
+    cudaStream_t stream = nullptr;
+    DevBuf<double>   X, psi;
+    DevBuf<uint32_t> cnt;
+    DevBuf<int>      status;
+    int              launches = 0;
+    cudaEvent_t      ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+gc_status validate_ksg(int natoms, int T, int k, const gc_opts& o, long* pb, long* pc)
+{
+    if (natoms < 2)
+        return fail(GC_ERR_INVALID, "kraskov_corrmatrix: need at least 2 atoms");
+    if (T <= k)
+        return fail(GC_ERR_INVALID, "kraskov_corrmatrix: nframes must exceed k (number of nearest neighbours)");
+    if (k < 1)
+        return fail(GC_ERR_INVALID, "kraskov_corrmatrix: k must be at least 1");
+    if (T > 65535)
+        return fail(GC_ERR_INVALID, "kraskov_corrmatrix: this build supports at most 65535 frames");
+    const long np = (long)natoms * (natoms - 1) / 2;
+    long       b = o.pair_begin, e = o.pair_end <= 0 ? np : o.pair_end;
+    if (b < 0 || b > e || e > np)
+        return fail(GC_ERR_INVALID, "pair shard out of range");
+    *pb = b;
+    *pc = e - b;
+    return GC_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+void gc_opts_init(gc_opts* o)
+{
+    if (!o)
+        return;
+    std::memset(o, 0, sizeof(*o));
+    o->device = -1;
+    o->path   = GC_PATH_AUTO;
+}
+
+const char* gc_last_error(void) { return g_last_error.c_str(); }
+
+int gc_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int gc_gpu_available(void)
+{
+    const int n = gc_device_count();
+    for (int d = 0; d < n; ++d)
+    {
+        cudaDeviceProp p{};
+        if (cudaGetDeviceProperties(&p, d) == cudaSuccess && p.major == 10)
+            return 1;
+    }
+    return 0;
+}
+
+gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts, gc_ksg_plan** out)
+{
+    if (!out)
+        return fail(GC_ERR_INVALID, "null plan output");
+    *out          = nullptr;
+    const gc_opts o = opts ? *opts : defaults();
+    long pb = 0, pc = 0;
+    GC_TRY(validate_ksg(natoms, nframes, k, o, &pb, &pc));
+    DeviceScope dev(o.device);
+    GC_TRY(dev.st);
+    std::unique_ptr<gc_ksg_plan> p(new gc_ksg_plan);
+    cudaGetDevice(&p->device);
+    p->natoms     = natoms;
+    p->T          = nframes;
+    p->K          = k;
+    p->path       = o.path;
+    p->pair_begin = pb;
+    p->pair_count = pc;
+    GC_TRY_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+    GC_TRY_CUDA(cudaEventCreate(&p->ev0));
+    GC_TRY_CUDA(cudaEventCreate(&p->ev1));
+    GC_TRY(p->X.alloc((size_t)3 * natoms * nframes));
+    GC_TRY(p->psi.alloc((size_t)nframes + 1));
+    GC_TRY(p->cnt.alloc((size_t)nframes * (size_t)(pc > 0 ? pc : 1)));
+    GC_TRY(p->status.alloc(1));
+    const std::vector<double> psi = digamma_table(nframes);
+    GC_TRY_CUDA(cudaMemcpy(p->psi.p, psi.data(), sizeof(double) * psi.size(), cudaMemcpyHostToDevice));
+    *out = p.release();
+    return GC_OK;
+}
+
+gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi, void* stream)
+{
+    if (!p || !d_xyz || !d_pair_mi)
+        return fail(GC_ERR_INVALID, "null plan or device buffer");
+    DeviceScope dev(p->device);
+    GC_TRY(dev.st);
+    cudaStream_t s = stream ? (cudaStream_t)stream : p->stream;
+    p->launches    = 0;
+    GC_TRY_CUDA(cudaMemsetAsync(p->status.p, 0, sizeof(int), s));
+    gc::launch_ksg_prepare(d_xyz, p->natoms, p->T, p->X.p, p->status.p, s);
+    ++p->launches;
+    if (p->pair_count > 0)
+    {
+        GC_TRY_CUDA(cudaEventRecord(p->ev0, s));
+        gc::launch_ksg_exact(p->X.p, p->T, p->K, p->pair_begin, p->pair_count, p->cnt.p, s);
+        GC_TRY_CUDA(cudaEventRecord(p->ev1, s));
+        gc::launch_ksg_finalize(p->cnt.p, p->pair_count, p->T, p->K, p->psi.p, d_pair_mi, s);
+        p->launches += 2;
+    }
+    GC_TRY_CUDA(cudaGetLastError());
+    return GC_OK;
+}
+
+gc_status gc_ksg_plan_sync(gc_ksg_plan* p)
+{
+    if (!p)
+        return fail(GC_ERR_INVALID, "null plan");
+    DeviceScope dev(p->device);
+    GC_TRY(dev.st);
+    GC_TRY_CUDA(cudaStreamSynchronize(p->stream));
+    GC_TRY_CUDA(cudaDeviceSynchronize());
+    int st = 0;
+    GC_TRY_CUDA(cudaMemcpy(&st, p->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    return status_to_error(st);
+}
+
+long gc_ksg_plan_pairs(const gc_ksg_plan* p) { return p ? p->pair_count : 0; }
+
+int gc_ksg_plan_launches(const gc_ksg_plan* p) { return p ? p->launches : 0; }
+
+float gc_ksg_plan_kernel_ms(const gc_ksg_plan* p)
+{
+    if (!p || !p->ev0 || !p->ev1 || p->pair_count <= 0)
+        return 0.0f;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, p->ev0, p->ev1) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return 0.0f;
+    }
+    return ms;
+}
+
+void gc_ksg_plan_destroy(gc_ksg_plan* p)
+{
+    if (!p)
+        return;
+    {
+        DeviceScope dev(p->device);
+        if (p->stream)
+            cudaStreamDestroy(p->stream);
+        if (p->ev0)
+            cudaEventDestroy(p->ev0);
+        if (p->ev1)
+            cudaEventDestroy(p->ev1);
+        p->X.reset();
+        p->psi.reset();
+        p->cnt.reset();
+        p->status.reset();
+    }
+    delete p;
+}
+
+gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, double* mi)
+{
+    GC_TRY(check_view(traj));
+    if (!mi)
+        return fail(GC_ERR_INVALID, "null output matrix");
+    const gc_opts o = opts ? *opts : defaults();
+    const int     n = traj->natoms, T = traj->nframes;
+    long          pb = 0, pc = 0;
+    GC_TRY(validate_ksg(n, T, k, o, &pb, &pc));
+    DeviceScope dev(o.device);
+    GC_TRY(dev.st);
+    gc_ksg_plan* raw = nullptr;
+    GC_TRY(gc_ksg_plan_create(n, T, k, &o, &raw));
+    std::unique_ptr<gc_ksg_plan, void (*)(gc_ksg_plan*)> plan(raw, gc_ksg_plan_destroy);
+    DevBuf<double> d_xyz, d_mi;
+    GC_TRY(d_xyz.alloc((size_t)n * T * 3));
+    GC_TRY(d_mi.alloc((size_t)(pc > 0 ? pc : 1)));
+    cudaStream_t s = plan->stream;
+    GC_TRY(upload_traj(traj, d_xyz.p, s));
+    GC_TRY(gc_ksg_plan_run(plan.get(), d_xyz.p, d_mi.p, s));
+    GC_TRY(gc_ksg_plan_sync(plan.get()));
+    std::vector<double> pm((size_t)pc);
+    if (pc > 0)
+        GC_TRY_CUDA(cudaMemcpy(pm.data(), d_mi.p, sizeof(double) * pc, cudaMemcpyDeviceToHost));
+    if (o.detail_nx || o.detail_ny)
+    {
+        std::vector<uint32_t> c((size_t)T * pc);
+        if (pc > 0)
+            GC_TRY_CUDA(cudaMemcpy(c.data(), plan->cnt.p, sizeof(uint32_t) * c.size(), cudaMemcpyDeviceToHost));
+        for (long pl = 0; pl < pc; ++pl)
+            for (int i = 0; i < T; ++i)
+            {
+                const uint32_t v = c[(size_t)i * pc + pl];
+                if (o.detail_nx)
+                    o.detail_nx[(size_t)pl * T + i] = (int32_t)(v & 0xFFFFu);
+                if (o.detail_ny)
+                    o.detail_ny[(size_t)pl * T + i] = (int32_t)(v >> 16);
+            }
+    }
+    // kraskov_corrmatrix: zero fill, diagonal 2000, symmetric entries.
+    std::memset(mi, 0, sizeof(double) * (size_t)n * n);
+    for (int a = 0; a < n; ++a)
+        mi[(size_t)a * n + a] = 2000.0;
+    for (long pl = 0; pl < pc; ++pl)
+    {
+        int a1, a2;
+        gc::pair_from_index(pb + pl, &a1, &a2);
+        mi[(size_t)a1 * n + a2] = pm[(size_t)pl];
+        mi[(size_t)a2 * n + a1] = pm[(size_t)pl];
+    }
+    return GC_OK;
+}
+
+gc_status gc_te_matrix(const gc_traj_view* traj, int k, int lag, const gc_opts* opts, double* te)
+{
+    GC_TRY(check_view(traj));
+    if (!te)
+        return fail(GC_ERR_INVALID, "null output matrix");
+    const gc_opts o = opts ? *opts : defaults();
+    const int     n = traj->natoms, T = traj->nframes;
+    if (k < 1)
+        return fail(GC_ERR_INVALID, "te_matrix: k must be at least 1");
+    if (lag < 0)
+        return fail(GC_ERR_INVALID, "te_matrix: lag must be non-negative");
+    std::memset(te, 0, sizeof(double) * (size_t)n * n);
+    const int Nv = T - lag;
+    if (Nv <= k)
+    {
+        std::fprintf(stderr, "Warning: TE: N_valid=%d <= k=%d; skipping.\n", Nv, k);
+        return GC_OK;
+    }
+    if (T > 65535)
+        return fail(GC_ERR_INVALID, "te_matrix: this build supports at most 65535 frames");
+    if (n < 2)
+        return GC_OK;
+    DeviceScope dev(o.device);
+    GC_TRY(dev.st);
+    StreamScope ss;
+    GC_TRY(ss.init(o.stream));
+    const long        np = (long)n * (n - 1);
+    DevBuf<double>    d_xyz, d_XT, d_psi, d_te;
+    DevBuf<uint2>     d_cnt;
+    DevBuf<int>       d_st;
+    GC_TRY(d_xyz.alloc((size_t)n * T * 3));
+    GC_TRY(d_XT.alloc((size_t)n * T * 3));
+    GC_TRY(d_psi.alloc((size_t)Nv + 1));
+    GC_TRY(d_te.alloc((size_t)n * n));
+    GC_TRY(d_cnt.alloc((size_t)Nv * np));
+    GC_TRY(d_st.alloc(1));
+    const std::vector<double> psi = digamma_table(Nv);
+    GC_TRY_CUDA(cudaMemcpyAsync(d_psi.p, psi.data(), sizeof(double) * psi.size(), cudaMemcpyHostToDevice, ss.s));
+    GC_TRY(upload_traj(traj, d_xyz.p, ss.s));
+    GC_TRY_CUDA(cudaMemsetAsync(d_st.p, 0, sizeof(int), ss.s));
+    GC_TRY_CUDA(cudaMemsetAsync(d_te.p, 0, sizeof(double) * (size_t)n * n, ss.s));
+    gc::launch_transpose_components(d_xyz.p, n, T, d_XT.p, d_st.p, ss.s);
+    gc::launch_te_exact(d_XT.p, n, T, k, lag, d_cnt.p, ss.s);
+    gc::launch_te_finalize(d_cnt.p, n, T, k, lag, d_psi.p, d_te.p, ss.s);
+    GC_TRY_CUDA(cudaGetLastError());
+    GC_TRY_CUDA(cudaStreamSynchronize(ss.s));
+    int st = 0;
+    GC_TRY_CUDA(cudaMemcpy(&st, d_st.p, sizeof(int), cudaMemcpyDeviceToHost));
+    GC_TRY(status_to_error(st & gc::kStatNonFinite));
+    GC_TRY_CUDA(cudaMemcpy(te, d_te.p, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToHost));
+    return GC_OK;
+}
+
+static gc_status gauss_like(const gc_traj_view* traj, const gc_opts* opts, double* mi, int mode)
+{
+    GC_TRY(check_view(traj));
+    if (!mi)
+        return fail(GC_ERR_INVALID, "null output matrix");
+    const gc_opts o = opts ? *opts : defaults();
+    const int     n = traj->natoms, T = traj->nframes;
+    if (mode == 1)
+    {
+        if (n < 2)
+            return fail(GC_ERR_INVALID, "gcmi_corrmatrix: need at least 2 atoms");
+        if (T < 6)
+            return fail(GC_ERR_INVALID, "gcmi_corrmatrix: need at least 6 frames for a non-singular 6x6 covariance");
+        if (T > 16384)
+            return fail(GC_ERR_INVALID, "gcmi_corrmatrix: this build supports at most 16384 frames");
+    }
+    else if (n < 1 || T < 1)
+        return fail(GC_ERR_INVALID, "gauss_corrmatrix: empty trajectory");
+    DeviceScope dev(o.device);
+    GC_TRY(dev.st);
+    StreamScope ss;
+    GC_TRY(ss.init(o.stream));
+    const long     nb = (long)n * (n + 1) / 2;
+    DevBuf<double> d_xyz, d_XF, d_Z, d_zt, d_blk, d_mat;
+    DevBuf<int>    d_st;
+    GC_TRY(d_xyz.alloc((size_t)n * T * 3));
+    GC_TRY(d_XF.alloc((size_t)n * T * 3));
+    GC_TRY(d_blk.alloc((size_t)nb * 9));
+    GC_TRY(d_mat.alloc((size_t)n * n));
+    GC_TRY(d_st.alloc(1));
+    if (mode == 1)
+    {
+        GC_TRY(d_Z.alloc((size_t)n * T * 3));
+        GC_TRY(d_zt.alloc((size_t)T));
+    }
+    GC_TRY(upload_traj(traj, d_xyz.p, ss.s));
+    GC_TRY_CUDA(cudaMemsetAsync(d_st.p, 0, sizeof(int), ss.s));
+    GC_TRY_CUDA(cudaMemsetAsync(d_mat.p, 0, sizeof(double) * (size_t)n * n, ss.s));
+    gc::launch_frame_major(d_xyz.p, n, T, d_XF.p, d_st.p, ss.s);
+    const double* V = d_XF.p;
+    if (mode == 1)
+    {
+        gc::launch_copula(d_XF.p, n, T, d_zt.p, d_Z.p, ss.s);
+        V = d_Z.p;
+    }
+    gc::launch_blocks(V, n, T, d_blk.p, ss.s);
+    const double log2pi = std::log(2.0 * 3.14159265358979323846);
+    gc::launch_pair_logdet(d_blk.p, n, T, mode, log2pi, d_mat.p, ss.s);
+    GC_TRY_CUDA(cudaGetLastError());
+    GC_TRY_CUDA(cudaStreamSynchronize(ss.s));
+    int st = 0;
+    GC_TRY_CUDA(cudaMemcpy(&st, d_st.p, sizeof(int), cudaMemcpyDeviceToHost));
+    GC_TRY(status_to_error(st & gc::kStatNonFinite));
+    GC_TRY_CUDA(cudaMemcpy(mi, d_mat.p, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToHost));
+    return GC_OK;
+}
+
+gc_status gc_gauss_matrix(const gc_traj_view* traj, const gc_opts* opts, double* mi)
+{
+    return gauss_like(traj, opts, mi, 0);
+}
+
+gc_status gc_gcmi_matrix(const gc_traj_view* traj, const gc_opts* opts, double* mi)
+{
+    return gauss_like(traj, opts, mi, 1);
+}
+
+
+gc_status gc_ksg_prepare(const gc_traj_view* traj, const gc_opts* opts, double* X, double* psi, double* scal)
+{
+    GC_TRY(check_view(traj));
+    if (!X || !psi)
+        return fail(GC_ERR_INVALID, "null output array");
+    const gc_opts o = opts ? *opts : defaults();
+    const int     n = traj->natoms, T = traj->nframes;
+    if (n < 1 || T < 2)
+        return fail(GC_ERR_INVALID, "kraskov_prepare: need at least one atom and two frames");
+    DeviceScope dev(o.device);
+    GC_TRY(dev.st);
+    StreamScope ss;
+    GC_TRY(ss.init(o.stream));
+    DevBuf<double> d_xyz, d_X;
+    DevBuf<int>    d_st;
+    GC_TRY(d_xyz.alloc((size_t)n * T * 3));
+    GC_TRY(d_X.alloc((size_t)n * T * 3));
+    GC_TRY(d_st.alloc(1));
+    GC_TRY(upload_traj(traj, d_xyz.p, ss.s));
+    GC_TRY_CUDA(cudaMemsetAsync(d_st.p, 0, sizeof(int), ss.s));
+    gc::launch_ksg_prepare(d_xyz.p, n, T, d_X.p, d_st.p, ss.s);
+    GC_TRY_CUDA(cudaGetLastError());
+    GC_TRY_CUDA(cudaStreamSynchronize(ss.s));
+    int st = 0;
+    GC_TRY_CUDA(cudaMemcpy(&st, d_st.p, sizeof(int), cudaMemcpyDeviceToHost));
+    GC_TRY(status_to_error(st));
+    GC_TRY_CUDA(cudaMemcpy(X, d_X.p, sizeof(double) * (size_t)n * T * 3, cudaMemcpyDeviceToHost));
+    const std::vector<double> tab = digamma_table(T);
+    std::memcpy(psi, tab.data(), sizeof(double) * tab.size());
+    if (scal)
+        for (int c = 0; c < 3 * n; ++c)
+        {
+            // X is min-shifted, so max - min is the row maximum.
+            double mx = 0.0;
+            for (int f = 0; f < T; ++f)
+                mx = X[(size_t)c * T + f] > mx ? X[(size_t)c * T + f] : mx;
+            scal[c] = (T - 5) / mx;
+        }
+    return GC_OK;
+}
+
+gc_status gc_ksg_pair(const double* rows6, int nframes, int k, const double* psi, const gc_opts* opts, double* mi)
+{
+    if (!rows6 || !psi || !mi)
+        return fail(GC_ERR_INVALID, "null argument");
+    const gc_opts o = opts ? *opts : defaults();
+    const int     T = nframes;
+    long          pb, pc;
+    gc_opts       one = o;
+    one.pair_begin = 0;
+    one.pair_end   = 0;
+    GC_TRY(validate_ksg(2, T, k, one, &pb, &pc));
+    DeviceScope dev(o.device);
+    GC_TRY(dev.st);
+    StreamScope ss;
+    GC_TRY(ss.init(o.stream));
+    // Two-atom system whose single pair (1, 0) has a1 = atom 1: the
+    // x-marginal (first three rows, the grid's first axis) goes to atom 1.
+    DevBuf<double>   d_X, d_psi, d_mi;
+    DevBuf<uint32_t> d_cnt;
+    GC_TRY(d_X.alloc((size_t)6 * T));
+    GC_TRY(d_psi.alloc((size_t)T + 1));
+    GC_TRY(d_mi.alloc(1));
+    GC_TRY(d_cnt.alloc((size_t)T));
+    GC_TRY_CUDA(cudaMemcpyAsync(d_X.p + (size_t)3 * T, rows6, sizeof(double) * 3 * T, cudaMemcpyHostToDevice, ss.s));
+    GC_TRY_CUDA(cudaMemcpyAsync(d_X.p, rows6 + (size_t)3 * T, sizeof(double) * 3 * T, cudaMemcpyHostToDevice, ss.s));
+    GC_TRY_CUDA(cudaMemcpyAsync(d_psi.p, psi, sizeof(double) * (T + 1), cudaMemcpyHostToDevice, ss.s));
+    gc::launch_ksg_exact(d_X.p, T, k, 0, 1, d_cnt.p, ss.s);
+    gc::launch_ksg_finalize(d_cnt.p, 1, T, k, d_psi.p, d_mi.p, ss.s);
+    GC_TRY_CUDA(cudaGetLastError());
+    GC_TRY_CUDA(cudaMemcpyAsync(mi, d_mi.p, sizeof(double), cudaMemcpyDeviceToHost, ss.s));
+    GC_TRY_CUDA(cudaStreamSynchronize(ss.s));
+    return GC_OK;
+}
+
+} // extern "C"

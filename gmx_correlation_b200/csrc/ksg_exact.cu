@@ -1,0 +1,245 @@
+// KSG (Kraskov algorithm 2) on B200: normalisation, the exact FP64
+// brute-force neighbour statistics, and the ordered MI reduction.
+//
+// Reference semantics (scdantu/gmx_correlation):
+//   kraskov_prepare  lib/kraskov.cpp:2168-2220
+//   mir_xnyn         lib/kraskov.cpp:1228-1331 (the estimator per pair)
+//   neiK / neiE      lib/kraskov.cpp:257-343 / :113-177 (exact k-NN, counts)
+//
+// For every (pair, query frame i) the exact kernel finds the k-th smallest
+// joint max-norm distance over j != i, breaks exact ties at that distance in
+// the reference's grid-scan order, takes eps_x / eps_y as the largest
+// marginal distance among the k chosen neighbours, and counts
+// n_x = #{j != i : d_x(i,j) <= eps_x} (same for y).  All distance
+// arithmetic is IEEE FP64 |a-b| and max, so every count equals the
+// reference's.  The counts are stored per query and reduced in frame order
+// by ksg_finalize_kernel, which reproduces mir_xnyn's summation exactly.
+
+#include "gc_common.cuh"
+#include "gc_internal.h"
+
+namespace gc {
+
+// One thread per component c = atom*3 + dim; sequential sums in frame
+// order with round-to-nearest intrinsics so no FMA contraction alters a
+// bit relative to the reference's plain double arithmetic.
+__global__ void ksg_prepare_kernel(const double* __restrict__ xyz, int natoms, int T,
+                                   double* __restrict__ X, int* __restrict__ status)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= natoms * 3)
+        return;
+    const int     atom = c / 3, d = c - 3 * (c / 3);
+    const double* src  = xyz + (size_t)atom * T * 3 + d;
+    double        me   = 0.0;
+    for (int f = 0; f < T; ++f)
+        me = __dadd_rn(me, src[(size_t)f * 3]);
+    me       = __ddiv_rn(me, (double)T);
+    double s = 0.0;
+    for (int f = 0; f < T; ++f)
+    {
+        const double t = __dsub_rn(src[(size_t)f * 3], me);
+        s              = __dadd_rn(s, __dmul_rn(t, t));
+    }
+    s = __ddiv_rn(s, (double)(T - 1));
+    s = __dsqrt_rn(s);
+    if (!isfinite(s))
+    {
+        atomicOr(status, kStatNonFinite);
+        return;
+    }
+    if (s == 0.0)
+    {
+        atomicOr(status, kStatZeroVariance);
+        return;
+    }
+    // min/max seeds of the reference: DBL_MAX/2 with its integer DBL_MAX.
+    double  mn = 1000000.0, mx = -1000000.0;
+    double* row = X + (size_t)c * T;
+    for (int f = 0; f < T; ++f)
+    {
+        const double z = __ddiv_rn(__dsub_rn(src[(size_t)f * 3], me), s);
+        row[f]         = z;
+        mn             = z < mn ? z : mn;
+        mx             = z > mx ? z : mx;
+    }
+    for (int f = 0; f < T; ++f)
+        row[f] = __dsub_rn(row[f], mn);
+}
+
+namespace {
+
+constexpr int kExactWarps = 8;
+constexpr int kExactQBlock = 64;
+
+struct PairRows
+{
+    const double* __restrict__ a0;
+    const double* __restrict__ a1;
+    const double* __restrict__ a2;
+    const double* __restrict__ b0;
+    const double* __restrict__ b1;
+    const double* __restrict__ b2;
+};
+
+} // namespace
+
+__global__ void __launch_bounds__(kExactWarps * 32)
+    ksg_exact_kernel(const double* __restrict__ X, int T, int K, long pair_begin, long pair_count,
+                     int nqb, int rank_shift, uint32_t* __restrict__ cnt)
+{
+    __shared__ unsigned hist[kExactWarps][256];
+    const int  warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long task = blockIdx.x;
+    const long pl   = task / nqb;
+    const int  qb   = (int)(task - pl * nqb);
+    if (pl >= pair_count)
+        return;
+    int a1, a2;
+    pair_from_index(pair_begin + pl, &a1, &a2);
+    PairRows r;
+    r.a0 = X + (size_t)(a1 * 3 + 0) * T;
+    r.a1 = X + (size_t)(a1 * 3 + 1) * T;
+    r.a2 = X + (size_t)(a1 * 3 + 2) * T;
+    r.b0 = X + (size_t)(a2 * 3 + 0) * T;
+    r.b1 = X + (size_t)(a2 * 3 + 1) * T;
+    r.b2 = X + (size_t)(a2 * 3 + 2) * T;
+    const ScanGrid g(ksg_box_count(T, K));
+    const int      i0 = qb * kExactQBlock;
+    const int      i1 = min(T, i0 + kExactQBlock);
+    unsigned*      h  = hist[warp];
+
+#pragma unroll 1
+    for (int i = i0 + warp; i < i1; i += kExactWarps)
+    {
+        const double qa0 = r.a0[i], qa1 = r.a1[i], qa2 = r.a2[i];
+        const double qb0 = r.b0[i], qb1 = r.b1[i], qb2 = r.b2[i];
+        auto dist = [&](int j, double& dx, double& dy) {
+            dx = fmax(fmax(fabs(qa0 - r.a0[j]), fabs(qa1 - r.a1[j])), fabs(qa2 - r.a2[j]));
+            dy = fmax(fmax(fabs(qb0 - r.b0[j]), fabs(qb1 - r.b1[j])), fabs(qb2 - r.b2[j]));
+        };
+        auto vkey = [&](int j, unsigned long long& k) -> bool {
+            if (j == i)
+                return false;
+            double dx, dy;
+            dist(j, dx, dy);
+            k = dbits(fmax(dx, dy));
+            return true;
+        };
+        int                      below;
+        const unsigned long long dkb  = warp_select_u64(vkey, T, K, 56, h, lane, &below);
+        const double             dk   = __longlong_as_double((long long)dkb);
+        const int                need = K - below;
+
+        int tied = 0;
+        for (int j = lane; j < T; j += 32)
+        {
+            if (j == i)
+                continue;
+            double dx, dy;
+            dist(j, dx, dy);
+            tied += fmax(dx, dy) == dk;
+        }
+        tied = __reduce_add_sync(kFull, tied);
+
+        const int          ix   = g.qcell(qa0), iy = g.qcell(qb0);
+        unsigned long long rcut = ~0ull;
+        if (tied > need)
+        {
+            auto rkey = [&](int j, unsigned long long& k) -> bool {
+                if (j == i)
+                    return false;
+                double dx, dy;
+                dist(j, dx, dy);
+                if (fmax(dx, dy) != dk)
+                    return false;
+                k = g.rank(ix, iy, r.a0[j], r.b0[j], j, T);
+                return true;
+            };
+            int b2;
+            rcut = warp_select_u64(rkey, T, need, rank_shift, h, lane, &b2);
+        }
+
+        double ex = 0.0, ey = 0.0;
+        for (int j = lane; j < T; j += 32)
+        {
+            if (j == i)
+                continue;
+            double dx, dy;
+            dist(j, dx, dy);
+            const double v  = fmax(dx, dy);
+            bool         in = v < dk;
+            if (!in && v == dk)
+                in = rcut == ~0ull || g.rank(ix, iy, r.a0[j], r.b0[j], j, T) <= rcut;
+            if (in)
+            {
+                ex = fmax(ex, dx);
+                ey = fmax(ey, dy);
+            }
+        }
+        ex = warp_max(ex);
+        ey = warp_max(ey);
+
+        int nx = 0, ny = 0;
+        for (int j = lane; j < T; j += 32)
+        {
+            if (j == i)
+                continue;
+            double dx, dy;
+            dist(j, dx, dy);
+            nx += dx <= ex;
+            ny += dy <= ey;
+        }
+        nx = __reduce_add_sync(kFull, nx);
+        ny = __reduce_add_sync(kFull, ny);
+        if (lane == 0)
+            cnt[(size_t)i * pair_count + pl] = (uint32_t)nx | ((uint32_t)ny << 16);
+    }
+}
+
+// MI = psi[N] + (psi[K] - 1/K) - (1/N) * sum_i (psi[n_x,i] + psi[n_y,i]),
+// summed over i in frame order (lib/kraskov.cpp:1262, :1303-1318).
+__global__ void ksg_finalize_kernel(const uint32_t* __restrict__ cnt, long pair_count, int T, int K,
+                                    const double* __restrict__ psi, double* __restrict__ pair_mi)
+{
+    const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (p >= pair_count)
+        return;
+    double s = 0.0;
+    for (int i = 0; i < T; ++i)
+    {
+        const uint32_t c = cnt[(size_t)i * pair_count + p];
+        s                = __dadd_rn(s, __dadd_rn(psi[c & 0xFFFFu], psi[c >> 16]));
+    }
+    const double phiK = __dsub_rn(psi[K], __ddiv_rn(1.0, (double)K));
+    const double dxy2 = __ddiv_rn(s, (double)T);
+    pair_mi[p]        = __dsub_rn(__dadd_rn(psi[T], phiK), dxy2);
+}
+
+void launch_ksg_prepare(const double* xyz, int natoms, int T, double* X, int* status, cudaStream_t s)
+{
+    const int n = natoms * 3;
+    ksg_prepare_kernel<<<(n + 127) / 128, 128, 0, s>>>(xyz, natoms, T, X, status);
+}
+
+void launch_ksg_exact(const double* X, int T, int K, long pair_begin, long pair_count, uint32_t* cnt,
+                      cudaStream_t s)
+{
+    const int  nqb   = (T + kExactQBlock - 1) / kExactQBlock;
+    const long tasks = pair_count * nqb;
+    const int  box   = ksg_box_count(T, K);
+    const unsigned long long maxrank = (unsigned long long)box * box * (unsigned long long)T;
+    int bits = 64 - __builtin_clzll(maxrank);
+    const int rank_shift = ((bits - 1) / 8) * 8;
+    ksg_exact_kernel<<<(unsigned)tasks, kExactWarps * 32, 0, s>>>(X, T, K, pair_begin, pair_count, nqb,
+                                                                  rank_shift, cnt);
+}
+
+void launch_ksg_finalize(const uint32_t* cnt, long pair_count, int T, int K, const double* psi,
+                         double* pair_mi, cudaStream_t s)
+{
+    ksg_finalize_kernel<<<(unsigned)((pair_count + 127) / 128), 128, 0, s>>>(cnt, pair_count, T, K, psi,
+                                                                            pair_mi);
+}
+
+} // namespace gc

@@ -1,0 +1,60 @@
+"""The C-ABI library loads and exports every entry point include/*.h declares
+(no compute calls: these run without a GPU)."""
+import ctypes
+import re
+
+import numpy as np
+import pytest
+
+from tests.conftest import ROOT
+
+
+def declared_functions():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        for m in re.finditer(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b(gc_\w+)\s*\(", text, flags=re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for must in ("gc_ksg_matrix", "gc_gauss_matrix", "gc_gcmi_matrix", "gc_te_matrix", "gc_pearsify",
+                 "gc_write_matrix", "gc_write_xpm", "gc_ksg_plan_create", "gc_last_error"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(gc):
+    L = ctypes.CDLL(str(gc.LIB_PATH))
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_opts_defaults(gc):
+    o = gc._Opts()
+    gc.lib().gc_opts_init(ctypes.byref(o))
+    assert o.device == -1 and o.path == 0 and o.pair_begin == 0 and o.pair_end == 0
+
+
+def test_invalid_arguments_fail_before_device(gc):
+    x = np.random.default_rng(0).normal(size=(1, 50, 3))
+    with pytest.raises(gc.GCError) as e:
+        gc.kraskov_corrmatrix(x, 5)
+    assert e.value.status == 1 and "at least 2 atoms" in str(e.value)
+    x = np.random.default_rng(0).normal(size=(3, 10, 3))
+    with pytest.raises(gc.GCError) as e:
+        gc.kraskov_corrmatrix(x, 10)
+    assert e.value.status == 1 and "nframes must exceed k" in str(e.value)
+    with pytest.raises(gc.GCError) as e:
+        gc.gcmi_corrmatrix(np.zeros((3, 5, 3)))
+    assert e.value.status == 1
+
+
+def test_no_device_is_an_error_not_a_fallback(gc):
+    if gc.lib().gc_device_count() > 0:
+        pytest.skip("a CUDA device is present")
+    x = np.random.default_rng(0).normal(size=(3, 40, 3))
+    with pytest.raises(gc.GCError) as e:
+        gc.kraskov_corrmatrix(x, 4)
+    assert e.value.status == 2

@@ -1,0 +1,127 @@
+"""KSG on the GPU against the reference's results: per-query counts n_x/n_y
+bit-exact and MI bit-identical (same counts, same digamma table, same
+frame-order summation), so max |dr| is 0 within the 6e-4 bar."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+R_TOL = 6e-4  # the reference's own CPU-vs-legacy gap (README.md:204)
+
+
+def pair_index(a1, a2):
+    return a1 * (a1 - 1) // 2 + a2
+
+
+@pytest.mark.parametrize("case", ["ties_q005", "box2"])
+@pytest.mark.parametrize("path", [0, 1])
+def test_golden_tie_cases(gc, golden, case, path):
+    g = golden[case]
+    mat, nx, ny = gc.kraskov_corrmatrix(g["x"], int(g["k"]), path=path, detail=True)
+    np.testing.assert_array_equal(nx, g["detail_nx"])
+    np.testing.assert_array_equal(ny, g["detail_ny"])
+    np.testing.assert_array_equal(mat, g["ksg"])
+
+
+@pytest.mark.parametrize("path", [0, 1])
+def test_small_config_bitwise(gc, golden, small_x, path):
+    g = golden["small"]
+    mat, nx, ny = gc.kraskov_corrmatrix(small_x, int(g["k"]), path=path, detail=True)
+    np.testing.assert_array_equal(mat, g["ksg"])
+    for p, (a1, a2) in enumerate(g["detail_pairs"]):
+        q = pair_index(int(a1), int(a2))
+        np.testing.assert_array_equal(nx[q], g["detail_nx"][p])
+        np.testing.assert_array_equal(ny[q], g["detail_ny"][p])
+    r_gpu, r_ref = gc.pearsify(mat.copy()), gc.pearsify(g["ksg"].copy())
+    assert np.max(np.abs(r_gpu - r_ref)) <= R_TOL
+
+
+def test_reference_size_sampled_pairs(gc, oracle):
+    """247 atoms x 2000 frames, k=100, float32-rounded positions: the full
+    GPU matrix, then 10 sampled pairs checked query by query."""
+    from gmx_correlation_b200.synth import config_traj
+    x = config_traj("ref")
+    k = 100
+    mat = gc.kraskov_corrmatrix(x, k)
+    assert mat.shape == (247, 247)
+    np.testing.assert_array_equal(np.diag(mat), 2000.0)
+    np.testing.assert_array_equal(mat, mat.T)
+    X, psi = oracle.prepare(x)
+    rng = np.random.default_rng(2024)
+    max_dr = 0.0
+    for _ in range(10):
+        a1 = int(rng.integers(1, 247))
+        a2 = int(rng.integers(0, a1))
+        d = oracle.ksg_pair_detail(X, psi, k, a1, a2)
+        p = pair_index(a1, a2)
+        _, nx, ny = gc.kraskov_corrmatrix(x, k, pairs=(p, p + 1), detail=True)
+        np.testing.assert_array_equal(nx[0], d["nx"])
+        np.testing.assert_array_equal(ny[0], d["ny"])
+        assert mat[a1, a2] == d["mi"]
+        r1 = gc.pearsify(np.array([[mat[a1, a2]]]))[0, 0]
+        r2 = gc.pearsify(np.array([[d["mi"]]]))[0, 0]
+        max_dr = max(max_dr, abs(r1 - r2))
+    assert max_dr <= R_TOL
+
+
+def test_shard_equals_full(gc, small_x):
+    full = gc.kraskov_corrmatrix(small_x, 10)
+    part = gc.kraskov_corrmatrix(small_x, 10, pairs=(100, 777))
+    n = small_x.shape[0]
+    for p in range(n * (n - 1) // 2):
+        a1 = int((1 + np.sqrt(1 + 8 * p)) // 2)
+        while a1 * (a1 - 1) // 2 > p:
+            a1 -= 1
+        while (a1 + 1) * a1 // 2 <= p:
+            a1 += 1
+        a2 = p - a1 * (a1 - 1) // 2
+        want = full[a1, a2] if 100 <= p < 777 else 0.0
+        assert part[a1, a2] == want and part[a2, a1] == want
+    np.testing.assert_array_equal(np.diag(part), 2000.0)
+
+
+def test_prepare_and_wrap_bitwise(gc, oracle, small_x):
+    X, psi, scal = gc.kraskov_prepare(small_x)
+    Xo, psio = oracle.prepare(small_x)
+    np.testing.assert_array_equal(X, Xo)
+    np.testing.assert_array_equal(psi, psio)
+    for a1, a2 in [(1, 0), (50, 3), (63, 62)]:
+        d = oracle.ksg_pair_detail(Xo, psio, 10, a1, a2)
+        assert gc.kraskov_wrap(X, psi, a1, a2, 10) == d["mi"]
+
+
+def test_device_resident_plan(gc, golden, small_x):
+    torch = pytest.importorskip("torch")
+    n, T = small_x.shape[0], small_x.shape[1]
+    d_xyz = torch.from_numpy(small_x).cuda()
+    plan = gc.KsgPlan(n, T, 10)
+    out = torch.zeros(plan.pairs, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        plan.run(d_xyz.data_ptr(), out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        plan.sync()
+    assert plan.launches >= 1 and plan.kernel_ms > 0
+    g = golden["small"]["ksg"]
+    want = np.array([g[a1, a2] for a1 in range(1, n) for a2 in range(a1)])  # p = a1(a1-1)/2 + a2
+    np.testing.assert_array_equal(out.cpu().numpy(), want)
+    plan.close()
+
+
+def test_bad_inputs_are_errors(gc, small_x):
+    x = small_x[:4].copy()
+    x[2, :, 1] = 0.0
+    with pytest.raises(gc.GCError) as e:
+        gc.kraskov_corrmatrix(x, 5)
+    assert e.value.status == 4
+    x = small_x[:4].copy()
+    x[1, 7, 0] = np.nan
+    with pytest.raises(gc.GCError) as e:
+        gc.kraskov_corrmatrix(x, 5)
+    assert e.value.status == 5
+
+
+def test_k_equal_to_frames_minus_one(gc, oracle):
+    from gmx_correlation_b200.synth import synth_traj
+    x = synth_traj(4, 40, 3, 0.1, seed=9)
+    np.testing.assert_array_equal(gc.kraskov_corrmatrix(x, 39), oracle.ksg_matrix(x, 39))
+    np.testing.assert_array_equal(gc.kraskov_corrmatrix(x, 1), oracle.ksg_matrix(x, 1))

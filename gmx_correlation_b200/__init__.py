@@ -96,6 +96,9 @@ def lib() -> ctypes.CDLL:
         L.gc_ksg_plan_pairs.argtypes = [ctypes.c_void_p]
         L.gc_ksg_plan_pairs.restype = ctypes.c_long
         L.gc_ksg_plan_launches.argtypes = [ctypes.c_void_p]
+        L.gc_ksg_plan_handoffs.argtypes = [ctypes.c_void_p]
+        L.gc_ksg_plan_handoffs.restype = ctypes.c_long
+        L.gc_ksg_plan_is_fast.argtypes = [ctypes.c_void_p]
         L.gc_ksg_plan_kernel_ms.argtypes = [ctypes.c_void_p]
         L.gc_ksg_plan_kernel_ms.restype = ctypes.c_float
         L.gc_probe_fp32.argtypes = [ctypes.c_int, dp, dp]
@@ -286,6 +289,15 @@ class KsgPlan:
 
     def sync(self) -> None:
         _check(lib().gc_ksg_plan_sync(self._h))
+
+    @property
+    def handoffs(self) -> int:
+        """Queries of the last run computed by the exact hand-over kernel."""
+        return int(lib().gc_ksg_plan_handoffs(self._h))
+
+    @property
+    def is_fast(self) -> bool:
+        return bool(lib().gc_ksg_plan_is_fast(self._h))
 
     @property
     def kernel_ms(self) -> float:

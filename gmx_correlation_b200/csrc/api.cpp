@@ -8,6 +8,7 @@
 #include "gmx_corr_b200.h"
 #include "gc_internal.h"
 #include "gc_geom.h"
+#include "ksg_fast.h"
 
 #include <cuda_runtime.h>
 
@@ -207,7 +208,7 @@ struct StreamScope
 
 struct gc_ksg_plan
 {
-    int          device = 0;
+    int          device = 0, sms = 148;
     int          natoms = 0, T = 0, K = 0, path = GC_PATH_AUTO;
     long         pair_begin = 0, pair_count = 0;
     cudaStream_t stream = nullptr;
@@ -216,6 +217,19 @@ struct gc_ksg_plan
     DevBuf<int>      status;
     int              launches = 0;
     cudaEvent_t      ev0 = nullptr, ev1 = nullptr;
+    // fast path workspace
+    bool                         fast = false;
+    int                          Q = 0, Lpad = 0, shift = 0, nb = 0, bufcap = 0;
+    DevBuf<float4>               X32;
+    DevBuf<float>                eps, S;
+    DevBuf<uint16_t>             P;
+    DevBuf<unsigned long long>   task_counter, queue;
+    DevBuf<unsigned>             queue_len;
+    unsigned                     queue_cap = 0;
+    long                         handoffs = 0;
+    const double*                last_xyz = nullptr;
+    double*                      last_mi  = nullptr;
+    cudaStream_t                 last_stream = nullptr;
 };
 
 namespace {
@@ -302,6 +316,30 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
     GC_TRY(p->psi.alloc((size_t)nframes + 1));
     GC_TRY(p->cnt.alloc((size_t)nframes * (size_t)(pc > 0 ? pc : 1)));
     GC_TRY(p->status.alloc(1));
+    GC_TRY_CUDA(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, p->device));
+    // The fast path sorts each marginal row in shared memory (<= 16384
+    // frames); longer trajectories use the exact kernels throughout.
+    p->fast = o.path != GC_PATH_EXACT_FP64 && nframes - 1 <= 16384 && pc > 0;
+    if (p->fast)
+    {
+        const int    T    = nframes;
+        p->Lpad           = ((T - 1) + 31) & ~31;
+        const double row  = (double)natoms * p->Lpad * 6.0;
+        const double budget = 8.0 * (1 << 30); // sorted rows of one query block
+        long         q    = (long)(budget / row);
+        p->Q              = (int)(q < 1 ? 1 : (q > T ? T : q));
+        gc::walk_histogram_shape(k, &p->shift, &p->nb);
+        p->bufcap = 1024;
+        GC_TRY(p->X32.alloc((size_t)natoms * T));
+        GC_TRY(p->eps.alloc((size_t)natoms));
+        GC_TRY(p->S.alloc((size_t)natoms * p->Q * p->Lpad));
+        GC_TRY(p->P.alloc((size_t)natoms * p->Q * p->Lpad));
+        GC_TRY(p->task_counter.alloc(1));
+        const double want = (double)pc * T;
+        p->queue_cap      = (unsigned)(want < 4194304.0 ? want : 4194304.0);
+        GC_TRY(p->queue.alloc(p->queue_cap));
+        GC_TRY(p->queue_len.alloc(1));
+    }
     const std::vector<double> psi = digamma_table(nframes);
     GC_TRY_CUDA(cudaMemcpy(p->psi.p, psi.data(), sizeof(double) * psi.size(), cudaMemcpyHostToDevice));
     *out = p.release();
@@ -319,13 +357,73 @@ gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi
     GC_TRY_CUDA(cudaMemsetAsync(p->status.p, 0, sizeof(int), s));
     gc::launch_ksg_prepare(d_xyz, p->natoms, p->T, p->X.p, p->status.p, s);
     ++p->launches;
+    p->last_xyz    = d_xyz;
+    p->last_mi     = d_pair_mi;
+    p->last_stream = s;
     if (p->pair_count > 0)
     {
         GC_TRY_CUDA(cudaEventRecord(p->ev0, s));
-        gc::launch_ksg_exact(p->X.p, p->T, p->K, p->pair_begin, p->pair_count, p->cnt.p, s);
+        if (p->fast)
+        {
+            const int T = p->T;
+            gc::launch_ksg_x32(p->X.p, p->natoms, T, p->X32.p, p->eps.p, s);
+            GC_TRY_CUDA(cudaMemsetAsync(p->queue_len.p, 0, sizeof(unsigned), s));
+            p->launches += 1;
+            gc::WalkParams w{};
+            w.X32 = p->X32.p;
+            w.X64 = p->X.p;
+            w.eps_atom = p->eps.p;
+            w.S = p->S.p;
+            w.P = p->P.p;
+            w.Lpad = p->Lpad;
+            w.T = T;
+            w.K = p->K;
+            w.box = gc::ksg_box_count(T, p->K);
+            w.pair_begin = p->pair_begin;
+            w.pair_count = p->pair_count;
+            w.shift = p->shift;
+            w.nb = p->nb;
+            w.bufcap = p->bufcap;
+            w.warp_smem = gc::walk_warp_smem(p->nb, p->bufcap);
+            w.cnt = p->cnt.p;
+            w.task_counter = p->task_counter.p;
+            w.queue = p->queue.p;
+            w.queue_len = p->queue_len.p;
+            w.queue_cap = p->queue_cap;
+            w.status = p->status.p;
+            for (int i0 = 0; i0 < T; i0 += p->Q)
+            {
+                const int Qb = T - i0 < p->Q ? T - i0 : p->Q;
+                gc::launch_ksg_rows(p->X32.p, p->natoms, T, i0, Qb, p->Lpad, p->S.p, p->P.p, s);
+                GC_TRY_CUDA(cudaMemsetAsync(p->task_counter.p, 0, sizeof(unsigned long long), s));
+                w.i0 = i0;
+                w.Q  = Qb;
+                gc::launch_ksg_walk(w, p->sms, s);
+                p->launches += 2;
+            }
+            gc::QueueParams qp{};
+            qp.X64 = p->X.p;
+            qp.T = T;
+            qp.K = p->K;
+            qp.box = w.box;
+            qp.rank_shift = gc::rank_top_shift(w.box, T);
+            qp.pair_begin = p->pair_begin;
+            qp.pair_count = p->pair_count;
+            qp.cnt = p->cnt.p;
+            qp.queue = p->queue.p;
+            qp.queue_len = p->queue_len.p;
+            qp.queue_cap = p->queue_cap;
+            gc::launch_ksg_queue(qp, p->sms, s);
+            p->launches += 1;
+        }
+        else
+        {
+            gc::launch_ksg_exact(p->X.p, p->T, p->K, p->pair_begin, p->pair_count, p->cnt.p, s);
+            p->launches += 1;
+        }
         GC_TRY_CUDA(cudaEventRecord(p->ev1, s));
         gc::launch_ksg_finalize(p->cnt.p, p->pair_count, p->T, p->K, p->psi.p, d_pair_mi, s);
-        p->launches += 2;
+        p->launches += 1;
     }
     GC_TRY_CUDA(cudaGetLastError());
     return GC_OK;
@@ -341,12 +439,34 @@ gc_status gc_ksg_plan_sync(gc_ksg_plan* p)
     GC_TRY_CUDA(cudaDeviceSynchronize());
     int st = 0;
     GC_TRY_CUDA(cudaMemcpy(&st, p->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    p->handoffs = 0;
+    if (p->fast)
+    {
+        unsigned h = 0;
+        GC_TRY_CUDA(cudaMemcpy(&h, p->queue_len.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        p->handoffs = (long)h;
+    }
+    if ((st & gc::kStatQueueOverflow) && p->last_mi && p->pair_count > 0)
+    {
+        // More hand-overs than the queue holds: recompute every query of the
+        // shard with the exact kernel (same results, slower).
+        cudaStream_t s = p->last_stream;
+        gc::launch_ksg_exact(p->X.p, p->T, p->K, p->pair_begin, p->pair_count, p->cnt.p, s);
+        gc::launch_ksg_finalize(p->cnt.p, p->pair_count, p->T, p->K, p->psi.p, p->last_mi, s);
+        GC_TRY_CUDA(cudaGetLastError());
+        GC_TRY_CUDA(cudaStreamSynchronize(s));
+        st &= ~gc::kStatQueueOverflow;
+    }
     return status_to_error(st);
 }
 
 long gc_ksg_plan_pairs(const gc_ksg_plan* p) { return p ? p->pair_count : 0; }
 
 int gc_ksg_plan_launches(const gc_ksg_plan* p) { return p ? p->launches : 0; }
+
+long gc_ksg_plan_handoffs(const gc_ksg_plan* p) { return p ? p->handoffs : 0; }
+
+int gc_ksg_plan_is_fast(const gc_ksg_plan* p) { return p && p->fast ? 1 : 0; }
 
 float gc_ksg_plan_kernel_ms(const gc_ksg_plan* p)
 {
@@ -377,6 +497,13 @@ void gc_ksg_plan_destroy(gc_ksg_plan* p)
         p->psi.reset();
         p->cnt.reset();
         p->status.reset();
+        p->X32.reset();
+        p->eps.reset();
+        p->S.reset();
+        p->P.reset();
+        p->task_counter.reset();
+        p->queue.reset();
+        p->queue_len.reset();
     }
     delete p;
 }

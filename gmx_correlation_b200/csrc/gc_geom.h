@@ -62,4 +62,13 @@ GC_HD inline long long scan_pos(int dxm, int dym, int bs)
     return base + 2 * h + (ry + h - 1);
 }
 
+// Highest byte offset a tie-break rank key (scan position * T + frame) can
+// use, for the radix selection over ranks (host only).
+inline int rank_top_shift(int box, int T)
+{
+    const unsigned long long maxrank = (unsigned long long)box * box * (unsigned long long)T;
+    const int                bits    = 64 - __builtin_clzll(maxrank);
+    return ((bits - 1) / 8) * 8;
+}
+
 } // namespace gc

@@ -15,7 +15,8 @@ enum : int
     kStatZeroVariance = 2,
     kStatFallback     = 4, // fast path handed queries to the exact repair kernel
     kStatTimeout      = 8,
-    kStatInternal     = 16
+    kStatInternal     = 16,
+    kStatQueueOverflow = 32 // more hand-overs than the queue holds: rerun exact
 };
 
 // ---- KSG -------------------------------------------------------------------

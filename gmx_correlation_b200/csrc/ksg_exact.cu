@@ -17,6 +17,7 @@
 
 #include "gc_common.cuh"
 #include "gc_internal.h"
+#include "ksg_exact_query.cuh"
 
 namespace gc {
 
@@ -68,25 +69,13 @@ __global__ void ksg_prepare_kernel(const double* __restrict__ xyz, int natoms, i
 }
 
 namespace {
-
-constexpr int kExactWarps = 8;
+constexpr int kExactWarps  = 8;
 constexpr int kExactQBlock = 64;
-
-struct PairRows
-{
-    const double* __restrict__ a0;
-    const double* __restrict__ a1;
-    const double* __restrict__ a2;
-    const double* __restrict__ b0;
-    const double* __restrict__ b1;
-    const double* __restrict__ b2;
-};
-
 } // namespace
 
 __global__ void __launch_bounds__(kExactWarps * 32)
-    ksg_exact_kernel(const double* __restrict__ X, int T, int K, long pair_begin, long pair_count,
-                     int nqb, int rank_shift, uint32_t* __restrict__ cnt)
+    ksg_exact_kernel(const double* __restrict__ X, int T, int K, long pair_begin, long pair_count, int nqb,
+                     int rank_shift, uint32_t* __restrict__ cnt)
 {
     __shared__ unsigned hist[kExactWarps][256];
     const int  warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -97,103 +86,15 @@ __global__ void __launch_bounds__(kExactWarps * 32)
         return;
     int a1, a2;
     pair_from_index(pair_begin + pl, &a1, &a2);
-    PairRows r;
-    r.a0 = X + (size_t)(a1 * 3 + 0) * T;
-    r.a1 = X + (size_t)(a1 * 3 + 1) * T;
-    r.a2 = X + (size_t)(a1 * 3 + 2) * T;
-    r.b0 = X + (size_t)(a2 * 3 + 0) * T;
-    r.b1 = X + (size_t)(a2 * 3 + 1) * T;
-    r.b2 = X + (size_t)(a2 * 3 + 2) * T;
-    const ScanGrid g(ksg_box_count(T, K));
-    const int      i0 = qb * kExactQBlock;
-    const int      i1 = min(T, i0 + kExactQBlock);
-    unsigned*      h  = hist[warp];
-
+    const int box = ksg_box_count(T, K);
+    const int i0  = qb * kExactQBlock;
+    const int i1  = min(T, i0 + kExactQBlock);
 #pragma unroll 1
     for (int i = i0 + warp; i < i1; i += kExactWarps)
     {
-        const double qa0 = r.a0[i], qa1 = r.a1[i], qa2 = r.a2[i];
-        const double qb0 = r.b0[i], qb1 = r.b1[i], qb2 = r.b2[i];
-        auto dist = [&](int j, double& dx, double& dy) {
-            dx = fmax(fmax(fabs(qa0 - r.a0[j]), fabs(qa1 - r.a1[j])), fabs(qa2 - r.a2[j]));
-            dy = fmax(fmax(fabs(qb0 - r.b0[j]), fabs(qb1 - r.b1[j])), fabs(qb2 - r.b2[j]));
-        };
-        auto vkey = [&](int j, unsigned long long& k) -> bool {
-            if (j == i)
-                return false;
-            double dx, dy;
-            dist(j, dx, dy);
-            k = dbits(fmax(dx, dy));
-            return true;
-        };
-        int                      below;
-        const unsigned long long dkb  = warp_select_u64(vkey, T, K, 56, h, lane, &below);
-        const double             dk   = __longlong_as_double((long long)dkb);
-        const int                need = K - below;
-
-        int tied = 0;
-        for (int j = lane; j < T; j += 32)
-        {
-            if (j == i)
-                continue;
-            double dx, dy;
-            dist(j, dx, dy);
-            tied += fmax(dx, dy) == dk;
-        }
-        tied = __reduce_add_sync(kFull, tied);
-
-        const int          ix   = g.qcell(qa0), iy = g.qcell(qb0);
-        unsigned long long rcut = ~0ull;
-        if (tied > need)
-        {
-            auto rkey = [&](int j, unsigned long long& k) -> bool {
-                if (j == i)
-                    return false;
-                double dx, dy;
-                dist(j, dx, dy);
-                if (fmax(dx, dy) != dk)
-                    return false;
-                k = g.rank(ix, iy, r.a0[j], r.b0[j], j, T);
-                return true;
-            };
-            int b2;
-            rcut = warp_select_u64(rkey, T, need, rank_shift, h, lane, &b2);
-        }
-
-        double ex = 0.0, ey = 0.0;
-        for (int j = lane; j < T; j += 32)
-        {
-            if (j == i)
-                continue;
-            double dx, dy;
-            dist(j, dx, dy);
-            const double v  = fmax(dx, dy);
-            bool         in = v < dk;
-            if (!in && v == dk)
-                in = rcut == ~0ull || g.rank(ix, iy, r.a0[j], r.b0[j], j, T) <= rcut;
-            if (in)
-            {
-                ex = fmax(ex, dx);
-                ey = fmax(ey, dy);
-            }
-        }
-        ex = warp_max(ex);
-        ey = warp_max(ey);
-
-        int nx = 0, ny = 0;
-        for (int j = lane; j < T; j += 32)
-        {
-            if (j == i)
-                continue;
-            double dx, dy;
-            dist(j, dx, dy);
-            nx += dx <= ex;
-            ny += dy <= ey;
-        }
-        nx = __reduce_add_sync(kFull, nx);
-        ny = __reduce_add_sync(kFull, ny);
+        const uint32_t c = exact_query(X, T, K, a1, a2, i, box, rank_shift, hist[warp], lane);
         if (lane == 0)
-            cnt[(size_t)i * pair_count + pl] = (uint32_t)nx | ((uint32_t)ny << 16);
+            cnt[(size_t)i * pair_count + pl] = c;
     }
 }
 
@@ -227,10 +128,7 @@ void launch_ksg_exact(const double* X, int T, int K, long pair_begin, long pair_
 {
     const int  nqb   = (T + kExactQBlock - 1) / kExactQBlock;
     const long tasks = pair_count * nqb;
-    const int  box   = ksg_box_count(T, K);
-    const unsigned long long maxrank = (unsigned long long)box * box * (unsigned long long)T;
-    int bits = 64 - __builtin_clzll(maxrank);
-    const int rank_shift = ((bits - 1) / 8) * 8;
+    const int  rank_shift = rank_top_shift(ksg_box_count(T, K), T);
     ksg_exact_kernel<<<(unsigned)tasks, kExactWarps * 32, 0, s>>>(X, T, K, pair_begin, pair_count, nqb,
                                                                   rank_shift, cnt);
 }

@@ -150,6 +150,11 @@ gc_status gc_ksg_plan_sync(gc_ksg_plan* plan);
 long gc_ksg_plan_pairs(const gc_ksg_plan* plan);
 /* Kernel launches issued by the last gc_ksg_plan_run. */
 int gc_ksg_plan_launches(const gc_ksg_plan* plan);
+/* 1 if the plan runs the FP32 fast path (0: exact FP64 kernels only). */
+int gc_ksg_plan_is_fast(const gc_ksg_plan* plan);
+/* Queries of the last run that the fast path handed to the exact FP64
+ * kernel (valid after gc_ksg_plan_sync). */
+long gc_ksg_plan_handoffs(const gc_ksg_plan* plan);
 /* Device time in milliseconds of the neighbour-statistics kernel(s) of the
  * last run, measured with CUDA events on the run's stream (valid after the
  * run has completed). */

@@ -64,6 +64,31 @@ def test_reference_size_sampled_pairs(gc, oracle):
     assert max_dr <= R_TOL
 
 
+def test_fast_path_reference_size(gc):
+    """The FP32 walk handles nearly every query itself and agrees with the
+    exact FP64 kernels on every pair of the 247 x 2000, k=100 matrix."""
+    torch = pytest.importorskip("torch")
+    from gmx_correlation_b200.synth import config_traj
+    x = config_traj("ref")
+    n, T = x.shape[0], x.shape[1]
+    d_xyz = torch.from_numpy(x).cuda()
+    fast = gc.KsgPlan(n, T, 100)
+    exact = gc.KsgPlan(n, T, 100, path=gc.PATH_EXACT_FP64)
+    assert fast.is_fast and not exact.is_fast
+    out_f = torch.zeros(fast.pairs, dtype=torch.float64, device="cuda")
+    out_e = torch.zeros_like(out_f)
+    s = torch.cuda.Stream()
+    fast.run(d_xyz.data_ptr(), out_f.data_ptr(), s.cuda_stream)
+    exact.run(d_xyz.data_ptr(), out_e.data_ptr(), s.cuda_stream)
+    torch.cuda.synchronize()
+    fast.sync()
+    exact.sync()
+    assert fast.handoffs < 0.01 * fast.pairs * T
+    np.testing.assert_array_equal(out_f.cpu().numpy(), out_e.cpu().numpy())
+    fast.close()
+    exact.close()
+
+
 def test_shard_equals_full(gc, small_x):
     full = gc.kraskov_corrmatrix(small_x, 10)
     part = gc.kraskov_corrmatrix(small_x, 10, pairs=(100, 777))
@@ -101,6 +126,7 @@ def test_device_resident_plan(gc, golden, small_x):
         torch.cuda.synchronize()
         plan.sync()
     assert plan.launches >= 1 and plan.kernel_ms > 0
+    assert plan.is_fast
     g = golden["small"]["ksg"]
     want = np.array([g[a1, a2] for a1 in range(1, n) for a2 in range(a1)])  # p = a1(a1-1)/2 + a2
     np.testing.assert_array_equal(out.cpu().numpy(), want)

@@ -102,6 +102,8 @@ def lib() -> ctypes.CDLL:
         L.gc_ksg_plan_kernel_ms.argtypes = [ctypes.c_void_p]
         L.gc_ksg_plan_kernel_ms.restype = ctypes.c_float
         L.gc_probe_fp32.argtypes = [ctypes.c_int, dp, dp]
+        L.gc_ksg_pair_mi_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_void_p, ctypes.c_void_p]
         L.gc_ksg_plan_destroy.argtypes = [ctypes.c_void_p]
         L.gc_ksg_plan_destroy.restype = None
         _ = ip
@@ -262,6 +264,14 @@ def read_matrix(path) -> np.ndarray:
     if n * n != len(vals):
         raise ValueError(f"{len(vals)} values do not form a square matrix")
     return np.array(vals).reshape(n, n).T
+
+
+def ksg_pair_mi_noalloc(d_xyz: int, natoms: int, nframes: int, k: int, d_pair_mi: int,
+                        stream: int = 0) -> None:
+    """Pair MI into caller-owned device memory with no device allocation
+    (natoms <= 64, nframes <= 1024); pointers are raw device addresses."""
+    _check(lib().gc_ksg_pair_mi_noalloc(ctypes.c_void_p(d_xyz), int(natoms), int(nframes), int(k),
+                                        ctypes.c_void_p(d_pair_mi), ctypes.c_void_p(stream or 0)))
 
 
 class KsgPlan:

@@ -202,6 +202,8 @@ struct StreamScope
 
 } // namespace
 
+void gc::set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
 // ---------------------------------------------------------------------------
 // KSG plan
 // ---------------------------------------------------------------------------

@@ -19,6 +19,9 @@ enum : int
     kStatQueueOverflow = 32 // more hand-overs than the queue holds: rerun exact
 };
 
+// Sets the calling thread's gc_last_error() text.
+void set_last_error(const char* msg);
+
 // ---- KSG -------------------------------------------------------------------
 // xyz [natoms][T][3] (mean-centred) -> X [3*natoms][T] normalised, min-shifted
 // (kraskov_prepare arithmetic), status bits on error.

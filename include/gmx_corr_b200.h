@@ -167,6 +167,24 @@ void gc_ksg_plan_destroy(gc_ksg_plan* plan);
  * denominator. */
 gc_status gc_probe_fp32(int device, double* mix_ops_per_s, double* fma_flops_per_s);
 
+/* ---- KSG without device allocation ---------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (a plugin whose host application owns all device memory through its
+ * own pool, or a latency-critical caller that cannot take cudaMalloc /
+ * cudaFree): computes the pair MI of every atom pair with the exact FP64 KSG
+ * kernels, taking all scratch from one fixed array of about 9.8 MB that the
+ * library holds on every device that loads it until the process exits.
+ * Limits: natoms <= 64, nframes <= 1024; larger calls fail with
+ * GC_ERR_INVALID.  d_xyz: device [natoms][nframes][3] mean-centred
+ * coordinates; d_pair_mi: device [natoms*(natoms-1)/2], pair order
+ * p = a1*(a1-1)/2 + a2 (a2 < a1); stream: cudaStream_t (NULL = the legacy
+ * default stream).  Runs on the calling thread's current device and returns
+ * after the work has finished (it synchronises the stream to check the
+ * input-status word).  The first call on a device looks up the array's
+ * device address, so it should come before any stream capture.  All calls
+ * share the one array: calls whose work overlaps on the GPU race. */
+gc_status gc_ksg_pair_mi_noalloc(const double* d_xyz, int natoms, int nframes, int k, double* d_pair_mi, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

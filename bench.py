@@ -243,6 +243,8 @@ def run_ours(args):
     clocks = sampler.stop()
     plan.sync()
     handoffs = plan.handoffs
+    walk_mean = plan.walk_mean
+    reasons = {k: v for k, v in plan.handoff_reasons.items() if v}
     total_ms = sum(step_ms)
     launches = plan.launches * args.steps
     if pg:
@@ -281,7 +283,8 @@ def run_ours(args):
                        "variant": "plain", "pairs_per_gpu": npairs,
                        "l2": "256 MiB flush between timed steps",
                        "path": "fp32 sorted-row walk + exact fp64 repair" if plan.is_fast else "exact-fp64 brute force",
-                       "handed_to_exact": handoffs, "queries": npairs * T},
+                       "handed_to_exact": handoffs, "queries": npairs * T,
+                       "walk_entries_per_query": round(walk_mean, 1), "handoff_reasons": reasons},
             "e2e": {"value": ws * npairs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(x.nbytes),
                     "d2h_bytes_per_step": int(npairs * 8)},
             "gpu_launches": launches,

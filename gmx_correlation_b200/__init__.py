@@ -99,6 +99,10 @@ def lib() -> ctypes.CDLL:
         L.gc_ksg_plan_handoffs.argtypes = [ctypes.c_void_p]
         L.gc_ksg_plan_handoffs.restype = ctypes.c_long
         L.gc_ksg_plan_is_fast.argtypes = [ctypes.c_void_p]
+        L.gc_ksg_plan_handoff_reason.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.gc_ksg_plan_handoff_reason.restype = ctypes.c_long
+        L.gc_ksg_plan_walk_mean.argtypes = [ctypes.c_void_p]
+        L.gc_ksg_plan_walk_mean.restype = ctypes.c_double
         L.gc_ksg_plan_kernel_ms.argtypes = [ctypes.c_void_p]
         L.gc_ksg_plan_kernel_ms.restype = ctypes.c_float
         L.gc_probe_fp32.argtypes = [ctypes.c_int, dp, dp]
@@ -304,6 +308,18 @@ class KsgPlan:
     def handoffs(self) -> int:
         """Queries of the last run computed by the exact hand-over kernel."""
         return int(lib().gc_ksg_plan_handoffs(self._h))
+
+    @property
+    def handoff_reasons(self) -> dict:
+        """Hand-overs of the last run by cause."""
+        names = {1: "walk_longer_than_buffer", 2: "kth_outside_histogram", 3: "band_too_wide",
+                 4: "ambiguous_set_too_large", 5: "too_many_max_candidates"}
+        return {v: int(lib().gc_ksg_plan_handoff_reason(self._h, k)) for k, v in names.items()}
+
+    @property
+    def walk_mean(self) -> float:
+        """Mean sorted-row entries walked per query in the last run."""
+        return float(lib().gc_ksg_plan_walk_mean(self._h))
 
     @property
     def is_fast(self) -> bool:

@@ -227,6 +227,10 @@ struct gc_ksg_plan
     DevBuf<uint16_t>             P;
     DevBuf<unsigned long long>   task_counter, queue;
     DevBuf<unsigned>             queue_len;
+    DevBuf<unsigned long long>   walk_elems;
+    DevBuf<unsigned>             reasons;
+    long                         reason_counts[8] = {};
+    double                       walk_mean = 0.0;
     unsigned                     queue_cap = 0;
     long                         handoffs = 0;
     const double*                last_xyz = nullptr;
@@ -331,7 +335,7 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
         long         q    = (long)(budget / row);
         p->Q              = (int)(q < 1 ? 1 : (q > T ? T : q));
         gc::walk_histogram_shape(k, &p->shift, &p->nb);
-        p->bufcap = 1024;
+        p->bufcap = 640; // walk buffer entries per warp; longer walks go to the exact kernel
         GC_TRY(p->X32.alloc((size_t)natoms * T));
         GC_TRY(p->eps.alloc((size_t)natoms));
         GC_TRY(p->S.alloc((size_t)natoms * p->Q * p->Lpad));
@@ -341,6 +345,8 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
         p->queue_cap      = (unsigned)(want < 4194304.0 ? want : 4194304.0);
         GC_TRY(p->queue.alloc(p->queue_cap));
         GC_TRY(p->queue_len.alloc(1));
+        GC_TRY(p->walk_elems.alloc(1));
+        GC_TRY(p->reasons.alloc(8));
     }
     const std::vector<double> psi = digamma_table(nframes);
     GC_TRY_CUDA(cudaMemcpy(p->psi.p, psi.data(), sizeof(double) * psi.size(), cudaMemcpyHostToDevice));
@@ -368,8 +374,10 @@ gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi
         if (p->fast)
         {
             const int T = p->T;
-            gc::launch_ksg_x32(p->X.p, p->natoms, T, p->X32.p, p->eps.p, s);
+            GC_TRY_CUDA(gc::launch_ksg_x32(p->X.p, p->natoms, T, p->X32.p, p->eps.p, s));
             GC_TRY_CUDA(cudaMemsetAsync(p->queue_len.p, 0, sizeof(unsigned), s));
+            GC_TRY_CUDA(cudaMemsetAsync(p->reasons.p, 0, 8 * sizeof(unsigned), s));
+            GC_TRY_CUDA(cudaMemsetAsync(p->walk_elems.p, 0, sizeof(unsigned long long), s));
             p->launches += 1;
             gc::WalkParams w{};
             w.X32 = p->X32.p;
@@ -393,14 +401,16 @@ gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi
             w.queue_len = p->queue_len.p;
             w.queue_cap = p->queue_cap;
             w.status = p->status.p;
+            w.walk_elems = p->walk_elems.p;
+            w.reasons    = p->reasons.p;
             for (int i0 = 0; i0 < T; i0 += p->Q)
             {
                 const int Qb = T - i0 < p->Q ? T - i0 : p->Q;
-                gc::launch_ksg_rows(p->X32.p, p->natoms, T, i0, Qb, p->Lpad, p->S.p, p->P.p, s);
+                GC_TRY_CUDA(gc::launch_ksg_rows(p->X32.p, p->natoms, T, i0, Qb, p->Lpad, p->S.p, p->P.p, s));
                 GC_TRY_CUDA(cudaMemsetAsync(p->task_counter.p, 0, sizeof(unsigned long long), s));
                 w.i0 = i0;
                 w.Q  = Qb;
-                gc::launch_ksg_walk(w, p->sms, s);
+                GC_TRY_CUDA(gc::launch_ksg_walk(w, p->sms, s));
                 p->launches += 2;
             }
             gc::QueueParams qp{};
@@ -415,7 +425,7 @@ gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi
             qp.queue = p->queue.p;
             qp.queue_len = p->queue_len.p;
             qp.queue_cap = p->queue_cap;
-            gc::launch_ksg_queue(qp, p->sms, s);
+            GC_TRY_CUDA(gc::launch_ksg_queue(qp, p->sms, s));
             p->launches += 1;
         }
         else
@@ -447,6 +457,13 @@ gc_status gc_ksg_plan_sync(gc_ksg_plan* p)
         unsigned h = 0;
         GC_TRY_CUDA(cudaMemcpy(&h, p->queue_len.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
         p->handoffs = (long)h;
+        unsigned long long we = 0;
+        GC_TRY_CUDA(cudaMemcpy(&we, p->walk_elems.p, sizeof(we), cudaMemcpyDeviceToHost));
+        p->walk_mean = (double)we / ((double)p->pair_count * p->T);
+        unsigned rc[8] = {};
+        GC_TRY_CUDA(cudaMemcpy(rc, p->reasons.p, sizeof(rc), cudaMemcpyDeviceToHost));
+        for (int r = 0; r < 8; ++r)
+            p->reason_counts[r] = (long)rc[r];
     }
     if ((st & gc::kStatQueueOverflow) && p->last_mi && p->pair_count > 0)
     {
@@ -467,6 +484,13 @@ long gc_ksg_plan_pairs(const gc_ksg_plan* p) { return p ? p->pair_count : 0; }
 int gc_ksg_plan_launches(const gc_ksg_plan* p) { return p ? p->launches : 0; }
 
 long gc_ksg_plan_handoffs(const gc_ksg_plan* p) { return p ? p->handoffs : 0; }
+
+double gc_ksg_plan_walk_mean(const gc_ksg_plan* p) { return p ? p->walk_mean : 0.0; }
+
+long gc_ksg_plan_handoff_reason(const gc_ksg_plan* p, int reason)
+{
+    return (p && reason >= 0 && reason < 8) ? p->reason_counts[reason] : 0;
+}
 
 int gc_ksg_plan_is_fast(const gc_ksg_plan* p) { return p && p->fast ? 1 : 0; }
 
@@ -506,6 +530,8 @@ void gc_ksg_plan_destroy(gc_ksg_plan* p)
         p->task_counter.reset();
         p->queue.reset();
         p->queue_len.reset();
+        p->walk_elems.reset();
+        p->reasons.reset();
     }
     delete p;
 }

@@ -79,50 +79,165 @@ __global__ void ksg_x32_kernel(const double* __restrict__ X64, int natoms, int T
     }
 }
 
-// One CTA per (atom, query): sort the marginal distances of the query's
-// row (T-1 values, self excluded) with their frames, as 64-bit keys
-// (distance bits << 32 | frame) in shared memory.
-__global__ void ksg_rows_kernel(const float4* __restrict__ X32, int T, int i0, int Q, int Lpad, int N2,
-                                float* __restrict__ S, uint16_t* __restrict__ P)
+// One CTA per (atom, query): the row's T-1 marginal distances (self
+// excluded), sorted ascending with their frames.  Keys are
+// (distance bits << 32 | frame); a bucket pass over the row's key range
+// (histogram, scan, scatter) leaves a few keys per bucket, which one thread
+// per bucket insertion-sorts.  A row with a crowded bucket (more than 64
+// equal-ish distances, e.g. duplicated frames) is sorted by a bitonic
+// network over the same buffer instead.
+constexpr int kRowsThreads = 256;
+
+__global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(const float4* __restrict__ X32, int T, int i0, int Q,
+                                                                int Lpad, int N2, int nbin, float* __restrict__ S,
+                                                                uint16_t* __restrict__ P)
 {
-    extern __shared__ unsigned long long keys[];
-    const int row  = blockIdx.x;
-    const int a    = row / Q;
-    const int iq   = row - a * Q;
-    const int i    = i0 + iq;
-    const float4 q = X32[(size_t)a * T + i];
-    for (int m = threadIdx.x; m < N2; m += blockDim.x)
+    extern __shared__ __align__(16) unsigned char rows_smem[];
+    unsigned long long* keys   = reinterpret_cast<unsigned long long*>(rows_smem);      // [N2] sorted output
+    unsigned long long* in     = keys + N2;                                             // [N2] unsorted (bucket path)
+    unsigned*           hist   = reinterpret_cast<unsigned*>(in + (nbin ? N2 : 0));     // [nbin]
+    unsigned*           cursor = hist + nbin;                                           // [nbin]
+    __shared__ unsigned red_min[kRowsThreads / 32], red_max[kRowsThreads / 32];
+    __shared__ int      crowded;
+
+    const int    row = blockIdx.x;
+    const int    a   = row / Q;
+    const int    iq  = row - a * Q;
+    const int    i   = i0 + iq;
+    const int    N   = T - 1;
+    const int    tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const float4 q   = X32[(size_t)a * T + i];
+
+    unsigned kmin = 0xFFFFFFFFu, kmax = 0u;
+    for (int m = tid; m < N; m += kRowsThreads)
     {
-        unsigned long long k = ~0ull;
-        if (m < T - 1)
-        {
-            const int j = m < i ? m : m + 1;
-            const float d = dist3f(q, X32[(size_t)a * T + j]);
-            k = ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)j;
-        }
-        keys[m] = k;
+        const int      j = m < i ? m : m + 1;
+        const unsigned k = __float_as_uint(dist3f(q, X32[(size_t)a * T + j]));
+        (nbin ? in : keys)[m] = ((unsigned long long)k << 32) | (unsigned)j;
+        kmin             = min(kmin, k);
+        kmax             = max(kmax, k);
+    }
+    for (int b = tid; b < nbin; b += kRowsThreads)
+        hist[b] = 0u;
+    if (tid == 0)
+        crowded = nbin == 0; // no bucket pass for very long rows
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        kmin = min(kmin, __shfl_xor_sync(kFull, kmin, o));
+        kmax = max(kmax, __shfl_xor_sync(kFull, kmax, o));
+    }
+    if (lane == 0)
+    {
+        red_min[warp] = kmin;
+        red_max[warp] = kmax;
     }
     __syncthreads();
-    for (int k = 2; k <= N2; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1)
+    kmin = red_min[0];
+    kmax = red_max[0];
+    for (int w = 1; w < kRowsThreads / 32; ++w)
+    {
+        kmin = min(kmin, red_min[w]);
+        kmax = max(kmax, red_max[w]);
+    }
+    // bucket = floor((key - kmin) * nbin / (kmax - kmin + 1)), in FP32: the
+    // conversion and the scaling are monotone, so buckets keep key order
+    const float scale = (float)nbin / ((float)(kmax - kmin) + 1.0f);
+    auto bin_of = [&](unsigned long long key) -> unsigned {
+        const unsigned b = (unsigned)((float)((unsigned)(key >> 32) - kmin) * scale);
+        return b < (unsigned)nbin ? b : (unsigned)nbin - 1;
+    };
+    // histogram
+    for (int m = tid; m < N && nbin; m += kRowsThreads)
+        atomicAdd(&hist[bin_of(in[m])], 1u);
+    __syncthreads();
+    // exclusive scan of hist into cursor (each thread a contiguous slice)
+    const int per = nbin / kRowsThreads; // 0 without a bucket pass
+    unsigned  loc = 0;
+    for (int e = 0; e < per; ++e)
+        loc += hist[tid * per + e];
+    unsigned incl = loc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const unsigned y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o)
+            incl += y;
+    }
+    if (lane == 31)
+        red_min[warp] = incl;
+    __syncthreads();
+    unsigned wbase = 0;
+    for (int w = 0; w < warp; ++w)
+        wbase += red_min[w];
+    unsigned run = wbase + incl - loc;
+    for (int e = 0; e < per; ++e)
+    {
+        const unsigned c       = hist[tid * per + e];
+        cursor[tid * per + e]  = run;
+        if (c > 64)
+            crowded = 1;
+        run += c;
+    }
+    __syncthreads();
+    // scatter
+    if (!crowded)
+        for (int m = tid; m < N; m += kRowsThreads)
         {
-            for (int t = threadIdx.x; t < (N2 >> 1); t += blockDim.x)
-            {
-                const int idx = ((t / j) * (j << 1)) + (t % j);
-                const int prt = idx + j;
-                const unsigned long long x = keys[idx], y = keys[prt];
-                const bool up = (idx & k) == 0;
-                if ((x > y) == up)
-                {
-                    keys[idx] = y;
-                    keys[prt] = x;
-                }
-            }
-            __syncthreads();
+            const unsigned long long k   = in[m];
+            const unsigned           pos = atomicAdd(&cursor[bin_of(k)], 1u);
+            keys[pos]                    = k;
         }
+    else if (nbin)
+        for (int m = tid; m < N; m += kRowsThreads)
+            keys[m] = in[m];
+    __syncthreads();
+    if (!crowded)
+    {
+        // cursor[b] now holds the end of bucket b; sort each bucket
+        for (int e = 0; e < per; ++e)
+        {
+            const int      b   = tid * per + e;
+            const unsigned end = cursor[b], beg = end - hist[b];
+            for (unsigned x = beg + 1; x < end; ++x)
+            {
+                const unsigned long long v = keys[x];
+                unsigned                 y = x;
+                while (y > beg && keys[y - 1] > v)
+                {
+                    keys[y] = keys[y - 1];
+                    --y;
+                }
+                keys[y] = v;
+            }
+        }
+        __syncthreads();
+    }
+    else
+    {
+        for (int m = N + tid; m < N2; m += kRowsThreads)
+            keys[m] = ~0ull;
+        __syncthreads();
+        for (int k = 2; k <= N2; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1)
+            {
+                for (int t = tid; t < (N2 >> 1); t += kRowsThreads)
+                {
+                    const int idx = ((t / j) * (j << 1)) + (t % j);
+                    const int prt = idx + j;
+                    const unsigned long long x = keys[idx], y = keys[prt];
+                    if ((x > y) == ((idx & k) == 0))
+                    {
+                        keys[idx] = y;
+                        keys[prt] = x;
+                    }
+                }
+                __syncthreads();
+            }
+    }
     float*    srow = S + (size_t)row * Lpad;
     uint16_t* prow = P + (size_t)row * Lpad;
-    for (int m = threadIdx.x; m < T - 1; m += blockDim.x)
+    for (int m = tid; m < N; m += kRowsThreads)
     {
         const unsigned long long k = keys[m];
         srow[m] = __uint_as_float((unsigned)(k >> 32));
@@ -133,7 +248,7 @@ __global__ void ksg_rows_kernel(const float4* __restrict__ X32, int T, int i0, i
 namespace {
 
 // Warp-wide count of sorted row values < t (strict) or <= t.
-__device__ __forceinline__ int warp_rank(const float* __restrict__ row, int n, float t, bool strict, int lane)
+__device__ __noinline__ int warp_rank(const float* __restrict__ row, int n, float t, bool strict, int lane)
 {
     int lo = 0, hi = n;
     while (hi - lo > 32)
@@ -167,42 +282,25 @@ __device__ __forceinline__ int warp_rank(const float* __restrict__ row, int n, f
     return lo + __popc(__ballot_sync(kFull, ok));
 }
 
-// n = #{j != i : d64(atom; i, j) <= t64} from the sorted FP32 row, exact.
-__device__ int count_le_exact(const float* __restrict__ row, const uint16_t* __restrict__ perm, int n,
-                              const double* __restrict__ X64, int atom, int T, int i, double t64, float eps,
-                              int lane)
-{
-    const float lo_t = __double2float_rd(__dsub_rd(t64, (double)eps));
-    const float hi_t = __double2float_ru(__dadd_ru(t64, (double)eps));
-    const int   lo   = warp_rank(row, n, lo_t, true, lane);
-    const int   hi   = warp_rank(row, n, hi_t, false, lane);
-    int         add  = 0;
-    for (int m = lo + lane; m < hi; m += 32)
-        add += dist3d(X64, atom, T, i, perm[m]) <= t64;
-    return lo + __reduce_add_sync(kFull, add);
-}
-
 __device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
 
-// Bitonic sort of one uint32 per lane, ascending.
-__device__ __forceinline__ unsigned warp_sort_u32(unsigned v, int lane)
+// Warp maximum of non-negative floats / doubles: their IEEE bit patterns
+// order like the values, so single-instruction integer reductions do it.
+__device__ __forceinline__ float warp_max_nn(float v)
 {
-#pragma unroll
-    for (int k = 2; k <= 32; k <<= 1)
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1)
-        {
-            const unsigned o    = __shfl_xor_sync(kFull, v, j);
-            const bool     up   = (lane & k) == 0;
-            const bool     low  = (lane & j) == 0;
-            const unsigned mn   = min(v, o), mxv = max(v, o);
-            v                   = (low == up) ? mn : mxv;
-        }
-    return v;
+    return __uint_as_float(__reduce_max_sync(kFull, __float_as_uint(v)));
+}
+
+__device__ __forceinline__ double warp_max_nn(double v)
+{
+    const unsigned long long b  = (unsigned long long)__double_as_longlong(v);
+    const unsigned           hi = __reduce_max_sync(kFull, (unsigned)(b >> 32));
+    const unsigned           lo = __reduce_max_sync(kFull, (unsigned)(b >> 32) == hi ? (unsigned)b : 0u);
+    return __longlong_as_double((long long)(((unsigned long long)hi << 32) | lo));
 }
 
 // Bitonic sort of (key_hi, key_lo, payload) per lane, ascending lexicographic.
-__device__ __forceinline__ void warp_sort_kv(unsigned long long& kh, unsigned long long& kl, int& pay, int lane)
+__device__ __noinline__ void warp_sort_kv(unsigned long long& kh, unsigned long long& kl, int& pay, int lane)
 {
 #pragma unroll
     for (int k = 2; k <= 32; k <<= 1)
@@ -227,24 +325,71 @@ __device__ __forceinline__ void warp_sort_kv(unsigned long long& kh, unsigned lo
 
 } // namespace
 
-__global__ void __launch_bounds__(kWalkWarps * 32) ksg_walk_kernel(WalkParams p)
-{
-    extern __shared__ unsigned char smem_raw[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* base = smem_raw + (size_t)warp * p.warp_smem;
-    unsigned*  hist = reinterpret_cast<unsigned*>(base);
-    float*     bsw  = reinterpret_cast<float*>(base + p.nb * 4);
-    float*     bdo  = bsw + p.bufcap;
-    uint16_t*  bj   = reinterpret_cast<uint16_t*>(bdo + p.bufcap);
-    unsigned*  list = reinterpret_cast<unsigned*>(base + walk_list_offset(p.nb, p.bufcap));
-    // list layout: [0,32) u32 band / amb frames, [32,64) f32 amb dx, [64,96) f32 amb dy
-    float*     ldx  = reinterpret_cast<float*>(list + 32);
-    float*     ldy  = reinterpret_cast<float*>(list + 64);
-    double*    l64  = reinterpret_cast<double*>(list + 96); // [0,32) dx64, [32,64) dy64
+namespace {
 
-    const int       T    = p.T, K = p.K, Llen = T - 1;
+// 4 consecutive sorted-row entries of lane `lane` in the 128-element walk
+// step starting at g0 (m = g0 + 4*lane + q), padded with NaN / frame 0 (a
+// NaN compares false with everything, so padding is never taken).
+__device__ __forceinline__ void load_step(const float* __restrict__ Sw, const uint16_t* __restrict__ Pw, int g0,
+                                          int Llen, int lane, float4& s4, uint2& j2)
+{
+    const int m0 = g0 + 4 * lane;
+    if (m0 + 3 < Llen)
+    {
+        s4 = *reinterpret_cast<const float4*>(Sw + m0);
+        j2 = *reinterpret_cast<const uint2*>(Pw + m0);
+    }
+    else
+    {
+        const float nan = __int_as_float(0x7fc00000);
+        float       v[4];
+        unsigned    j[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+        {
+            v[q] = m0 + q < Llen ? Sw[m0 + q] : nan;
+            j[q] = m0 + q < Llen ? Pw[m0 + q] : 0u;
+        }
+        s4 = make_float4(v[0], v[1], v[2], v[3]);
+        j2 = make_uint2(j[0] | (j[1] << 16), j[2] | (j[3] << 16));
+    }
+}
+
+__device__ __forceinline__ float f4get(const float4& v, int q)
+{
+    return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+}
+
+__device__ __forceinline__ unsigned u2get16(const uint2& v, int q)
+{
+    return q < 2 ? ((v.x >> (16 * q)) & 0xFFFFu) : ((v.y >> (16 * (q - 2))) & 0xFFFFu);
+}
+
+} // namespace
+
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) ksg_walk_kernel(WalkParams p)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int      warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* base = smem_raw + (size_t)warp * p.warp_smem;
+    unsigned*      hist = reinterpret_cast<unsigned*>(base);
+    float*         bsw  = reinterpret_cast<float*>(base + p.nb * 4);
+    float*         bdo  = bsw + p.bufcap;
+    uint16_t*      bj   = reinterpret_cast<uint16_t*>(bdo + p.bufcap);
+    unsigned char* lst  = base + walk_list_offset(p.nb, p.bufcap);
+    float*         bv   = reinterpret_cast<float*>(lst);          // [64] band values
+    unsigned*      bjj  = reinterpret_cast<unsigned*>(lst + 256); // [64] band frames
+    float*         bdx  = reinterpret_cast<float*>(lst + 512);    // [64]
+    float*         bdy  = reinterpret_cast<float*>(lst + 768);    // [64]
+    unsigned*      aj   = reinterpret_cast<unsigned*>(lst + 1024); // [32] ambiguous: band slot
+    unsigned*      cj   = reinterpret_cast<unsigned*>(lst + 1152); // [32] max candidates: frames
+    double*        a64  = reinterpret_cast<double*>(lst + 1280);   // [64] ambiguous dx64 | dy64
+
+    const int       T = p.T, K = p.K, Llen = T - 1;
     const ScanGrid  grid(p.box);
     const long long total = (long long)p.Q * p.pair_count;
+    const float     inf   = __int_as_float(0x7f800000);
 
     for (;;)
     {
@@ -255,13 +400,28 @@ __global__ void __launch_bounds__(kWalkWarps * 32) ksg_walk_kernel(WalkParams p)
         if (t0 >= total)
             break;
         const long long t1 = min(total, t0 + 32);
+        int             iq = (int)(t0 / p.pair_count);
+        long            pl = (long)(t0 - (long long)iq * p.pair_count);
+        int             a1, a2;
+        pair_from_index(p.pair_begin + pl, &a1, &a2);
         for (long long t = t0; t < t1; ++t)
         {
-            const int  iq = (int)(t / p.pair_count);
-            const long pl = (long)(t - (long long)iq * p.pair_count);
-            const int  i  = p.i0 + iq;
-            int        a1, a2;
-            pair_from_index(p.pair_begin + pl, &a1, &a2);
+            if (t > t0)
+            {
+                // advance to the next pair (p = a1*(a1-1)/2 + a2 order)
+                if (++pl == p.pair_count)
+                {
+                    pl = 0;
+                    ++iq;
+                    pair_from_index(p.pair_begin, &a1, &a2);
+                }
+                else if (++a2 == a1)
+                {
+                    ++a1;
+                    a2 = 0;
+                }
+            }
+            const int       i  = p.i0 + iq;
             const float*    Sa = p.S + ((size_t)a1 * p.Q + iq) * p.Lpad;
             const float*    Sb = p.S + ((size_t)a2 * p.Q + iq) * p.Lpad;
             const uint16_t* Pa = p.P + ((size_t)a1 * p.Q + iq) * p.Lpad;
@@ -271,54 +431,75 @@ __global__ void __launch_bounds__(kWalkWarps * 32) ksg_walk_kernel(WalkParams p)
             const int       o  = wx ? a2 : a1;
             const float*    Sw = wx ? Sa : Sb;
             const uint16_t* Pw = wx ? Pa : Pb;
+            const float*    So = wx ? Sb : Sa;
+            const uint16_t* Po = wx ? Pb : Pa;
             const float     L  = wx ? Ra : Rb;
             const unsigned  Lb = __float_as_uint(L);
             const float4    xo = p.X32[(size_t)o * T + i];
-            const float*    X32o = reinterpret_cast<const float*>(p.X32 + (size_t)o * T);
+            const float4*   X32o = p.X32 + (size_t)o * T;
             const float     ea = p.eps_atom[a1], eb = p.eps_atom[a2];
+            const float     ew = wx ? ea : eb, eo = wx ? eb : ea;
             const float     e2 = __fmul_ru(2.0f, fmaxf(ea, eb));
-            bool            handoff = false;
+            // probes of the other atom's row for its count (every 64th entry)
+            const int   pr0 = (lane + 1) * 64 - 1, pr1 = (lane + 33) * 64 - 1;
+            const float probe0 = pr0 < Llen ? So[pr0] : inf;
+            const float probe1 = pr1 < Llen ? So[pr1] : inf;
+            bool        handoff = false;
 
-            for (int b = lane; b < p.nb; b += 32)
-                hist[b] = 0u;
+            for (int b = 4 * lane; b < p.nb; b += 128)
+                *reinterpret_cast<uint4*>(hist + b) = make_uint4(0u, 0u, 0u, 0u);
             __syncwarp();
 
-            // ---- pass 1: walk + histogram ------------------------------------
+            // ---- pass 1: walk in 128-entry steps + histogram -------------------
+            // Branch-free step: every lane gathers all four coordinates (padding
+            // entries read frame 0) and the taken mask only gates the counters.
             int      cnt_lo = 0, R = 0, m_end = 0;
-            unsigned thr    = 0;
-            float    stop   = __int_as_float(0x7f800000);
-            for (int base0 = 0; base0 < Llen; base0 += 32)
+            unsigned thr  = 0;
+            float    stop = inf;
+            float4   s4;
+            uint2    j2;
+            load_step(Sw, Pw, 0, Llen, lane, s4, j2);
+            for (int g0 = 0; g0 < Llen; g0 += 128)
             {
-                const int  m     = base0 + lane;
-                const bool valid = m < Llen;
-                const float sw   = valid ? Sw[m] : __int_as_float(0x7f800000);
-                if (__shfl_sync(kFull, sw, 0) > stop)
+                if (!(__shfl_sync(kFull, s4.x, 0) <= stop))
                     break;
-                const bool take = valid && sw <= stop;
-                float      Do   = 0.0f;
-                int        j    = 0;
-                if (take)
+                float4 ns4 = make_float4(nanf(""), nanf(""), nanf(""), nanf(""));
+                uint2  nj2 = make_uint2(0u, 0u);
+                if (g0 + 128 < Llen)
+                    load_step(Sw, Pw, g0 + 128, Llen, lane, ns4, nj2);
+                const float4 x0 = X32o[j2.x & 0xFFFFu], x1 = X32o[j2.x >> 16];
+                const float4 x2 = X32o[j2.y & 0xFFFFu], x3 = X32o[j2.y >> 16];
+                const float  d0 = dist3f(xo, x0), d1 = dist3f(xo, x1), d2 = dist3f(xo, x2), d3 = dist3f(xo, x3);
+                const float  sv[4] = {s4.x, s4.y, s4.z, s4.w};
+                const float  dv[4] = {d0, d1, d2, d3};
+                int          nlo = 0, ntk = 0;
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
                 {
-                    j  = Pw[m];
-                    Do = dist3f(xo, *reinterpret_cast<const float4*>(X32o + 4 * (size_t)j));
-                    if (m < p.bufcap)
-                    {
-                        bsw[m] = sw;
-                        bdo[m] = Do;
-                        bj[m]  = (uint16_t)j;
-                    }
+                    const float    v    = fmaxf(sv[q], dv[q]);
+                    const bool     take = sv[q] <= stop;
+                    const bool     lo   = take && v < L;
+                    const unsigned b    = min((__float_as_uint(v) - Lb) >> p.shift, (unsigned)p.nb - 1);
+                    nlo += lo;
+                    ntk += take;
+                    if (take && !lo)
+                        atomicAdd(&hist[b], 1u);
                 }
-                const float    v     = fmaxf(sw, Do);
-                const bool     below = take && v < L;
-                cnt_lo += __popc(__ballot_sync(kFull, below));
-                if (take && !below)
-                    atomicAdd(&hist[min((__float_as_uint(v) - Lb) >> p.shift, (unsigned)p.nb - 1)], 1u);
-                const unsigned tm = __ballot_sync(kFull, take);
-                m_end = base0 + __popc(tm);
-                __syncwarp();
-                if (stop == __int_as_float(0x7f800000))
+                const int m0 = g0 + 4 * lane;
+                if (m0 < p.bufcap)
                 {
-                    const float sl = __shfl_sync(kFull, sw, 31 - __clz(tm));
+                    *reinterpret_cast<float4*>(bsw + m0) = s4;
+                    *reinterpret_cast<float4*>(bdo + m0) = make_float4(d0, d1, d2, d3);
+                    *reinterpret_cast<uint2*>(bj + m0)   = j2;
+                }
+                cnt_lo += __reduce_add_sync(kFull, nlo);
+                const int ntake = __reduce_add_sync(kFull, ntk);
+                m_end           = g0 + ntake;
+                __syncwarp();
+                if (stop == inf && ntake > 0)
+                {
+                    const int   last = ntake - 1; // taken entries form a prefix of the step
+                    const float sl   = __shfl_sync(kFull, f4get(s4, last & 3), last >> 2);
                     if (sl >= L)
                     {
                         const unsigned bn  = min((__float_as_uint(sl) - Lb) >> p.shift, (unsigned)p.nb - 1);
@@ -331,200 +512,357 @@ __global__ void __launch_bounds__(kWalkWarps * 32) ksg_walk_kernel(WalkParams p)
                             stop = __fadd_ru(__uint_as_float(Lb + (bn << p.shift)), e2);
                     }
                 }
+                s4 = ns4;
+                j2 = nj2;
+            }
+            if (p.walk_elems && lane == 0)
+                atomicAdd(p.walk_elems, (unsigned long long)m_end);
+            // a walk longer than the buffer goes to the exact kernel (rare)
+            int reason = 0;
+            if (m_end > p.bufcap)
+                reason = 1;
+            handoff = reason != 0;
+
+
+            // ---- bucket of the k-th value: one warp scan over nb/32 buckets/lane
+            int bstar = -1;
+            {
+                const int per = p.nb >> 5; // 2..8 buckets per lane
+                unsigned  c[8];
+                unsigned  own = 0;
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                {
+                    c[e] = e < per ? hist[lane * per + e] : 0u;
+                    own += c[e];
+                }
+                unsigned incl = own;
+#pragma unroll
+                for (int sft = 1; sft < 32; sft <<= 1)
+                {
+                    const unsigned y = __shfl_up_sync(kFull, incl, sft);
+                    if (lane >= sft)
+                        incl += y;
+                }
+                const unsigned need  = (unsigned)(K - cnt_lo);
+                const unsigned excl  = incl - own;
+                const bool     here  = excl < need && need <= incl;
+                int            mine  = -1;
+                if (here)
+                {
+                    unsigned acc = excl;
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        if (mine < 0 && e < per)
+                        {
+                            acc += c[e];
+                            if (acc >= need)
+                                mine = lane * per + e;
+                        }
+                }
+                const unsigned who = __ballot_sync(kFull, here);
+                bstar              = who ? __shfl_sync(kFull, mine, __ffs(who) - 1) : -1;
+            }
+            if (!handoff && (bstar < 0 || bstar >= p.nb - 1))
+            {
+                handoff = true;
+                reason  = 2;
             }
 
-            // element m of the walk (buffered, or re-derived past the buffer)
-            auto elem = [&](int m, float& sw, float& Do, int& j) {
-                if (m < p.bufcap)
+            // ---- one pass: certain members, and the band around bucket bstar ----
+            // v < inlo: certainly among the k nearest (d32 >= lower bucket edge);
+            // inlo <= v <= bandhi: the band, which holds the k-th value and every
+            // entry within 2 eps of it; above bandhi: certainly not.
+            const double* xa = p.X64 + (size_t)a1 * 3 * T;
+            const double* xb = p.X64 + (size_t)a2 * 3 * T;
+            float mx = 0.0f, my = 0.0f, inlo = 0.0f, bandhi = 0.0f;
+            int   n_in = 0, nband = 0;
+            if (!handoff)
+            {
+                inlo   = __fsub_rd(__uint_as_float(Lb + ((unsigned)bstar << p.shift)), e2);
+                bandhi = __fadd_ru(__uint_as_float(Lb + ((unsigned)(bstar + 1) << p.shift)), e2);
+                int cin = 0;
+                for (int b0 = 0; b0 < m_end; b0 += 128)
                 {
-                    sw = bsw[m];
-                    Do = bdo[m];
-                    j  = bj[m];
+                    const int    m0 = b0 + 4 * lane;
+                    const int    mc = min(m0, p.bufcap - 4);
+                    const float4 a  = *reinterpret_cast<const float4*>(bsw + mc);
+                    const float4 d  = *reinterpret_cast<const float4*>(bdo + mc);
+                    const float  sv[4] = {a.x, a.y, a.z, a.w};
+                    const float  dv[4] = {d.x, d.y, d.z, d.w};
+                    bool         bd[4];
+                    bool         anyb = false;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                    {
+                        const float v  = fmaxf(sv[q], dv[q]);
+                        const bool  ok = m0 + q < m_end;
+                        const bool  in = ok && v < inlo;
+                        bd[q]          = ok && !in && v <= bandhi;
+                        anyb |= bd[q];
+                        mx = in ? fmaxf(mx, wx ? sv[q] : dv[q]) : mx;
+                        my = in ? fmaxf(my, wx ? dv[q] : sv[q]) : my;
+                        cin += in;
+                    }
+                    if (__any_sync(kFull, anyb))
+                    {
+                        const uint2 j = *reinterpret_cast<const uint2*>(bj + mc);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                        {
+                            const unsigned bm = __ballot_sync(kFull, bd[q]);
+                            const int      sl = nband + __popc(bm & lanemask_lt(lane));
+                            if (bd[q] && sl < 64)
+                            {
+                                bv[sl]  = fmaxf(sv[q], dv[q]);
+                                bjj[sl] = u2get16(j, q);
+                                bdx[sl] = wx ? sv[q] : dv[q];
+                                bdy[sl] = wx ? dv[q] : sv[q];
+                            }
+                            nband += __popc(bm);
+                        }
+                    }
+                }
+                n_in = __reduce_add_sync(kFull, cin);
+                if (nband > 64 || K - n_in < 1 || K - n_in > nband)
+                {
+                    handoff = true;
+                    reason  = 3;
+                }
+                __syncwarp();
+            }
+
+            // ---- the k-th value from the band, then exact members and the
+            //      ambiguous set (within 2 eps of it) ------------------------------
+            int   n_amb = 0;
+            float lower = 0.0f;
+            if (!handoff)
+            {
+                const int r = K - n_in; // 1-based rank of the k-th value in the band
+                float     d32 = 0.0f;
+                if (nband <= 32)
+                {
+                    const float mine = lane < nband ? bv[lane] : inf;
+                    int         rk   = 0;
+                    for (int f = 0; f < nband; ++f)
+                    {
+                        const float u = __shfl_sync(kFull, mine, f);
+                        rk += u < mine || (u == mine && f < lane);
+                    }
+                    const unsigned hit = __ballot_sync(kFull, lane < nband && rk == r - 1);
+                    d32                = __shfl_sync(kFull, mine, __ffs(hit) - 1);
                 }
                 else
                 {
-                    sw = Sw[m];
-                    j  = Pw[m];
-                    Do = dist3f(xo, *reinterpret_cast<const float4*>(X32o + 4 * (size_t)j));
-                }
-            };
-
-            // ---- pass 2: bucket of the k-th value, then the band ---------------
-            int acc = cnt_lo, bstar = -1, belowk = 0;
-            for (int b0 = 0; b0 < p.nb; b0 += 32)
-            {
-                const unsigned c    = hist[b0 + lane];
-                unsigned       incl = c;
-#pragma unroll
-                for (int s = 1; s < 32; s <<= 1)
-                {
-                    const unsigned y = __shfl_up_sync(kFull, incl, s);
-                    if (lane >= s)
-                        incl += y;
-                }
-                const unsigned tot = __shfl_sync(kFull, incl, 31);
-                if (acc + (int)tot >= K)
-                {
-                    const bool here = acc + (int)(incl - c) < K && acc + (int)incl >= K;
-                    const int  src  = __ffs(__ballot_sync(kFull, here)) - 1;
-                    bstar           = b0 + src;
-                    belowk          = acc + (int)__shfl_sync(kFull, incl - c, src);
-                    break;
-                }
-                acc += (int)tot;
-            }
-            const int nband = bstar >= 0 ? (int)hist[bstar] : 0;
-            if (bstar < 0 || bstar == p.nb - 1 || nband > 32)
-                handoff = true;
-
-            float d32 = 0.0f;
-            if (!handoff)
-            {
-                int nb_seen = 0;
-                for (int base0 = 0; base0 < m_end; base0 += 32)
-                {
-                    const int m = base0 + lane;
-                    float     sw = 0.0f, Do = 0.0f;
-                    int       j  = 0;
-                    bool      in = false;
-                    if (m < m_end)
+                    for (int e = lane; e < nband; e += 32)
                     {
-                        elem(m, sw, Do, j);
-                        const float v = fmaxf(sw, Do);
-                        in = v >= L && min((__float_as_uint(v) - Lb) >> p.shift, (unsigned)p.nb - 1) == (unsigned)bstar;
+                        const float v  = bv[e];
+                        int         rk = 0;
+                        for (int f = 0; f < nband; ++f)
+                        {
+                            const float u = bv[f];
+                            rk += u < v || (u == v && f < e);
+                        }
+                        if (rk == r - 1)
+                            d32 = v;
                     }
-                    const unsigned bm = __ballot_sync(kFull, in);
-                    const int      sl = nb_seen + __popc(bm & lanemask_lt(lane));
-                    if (in && sl < 32)
-                        list[sl] = __float_as_uint(fmaxf(sw, Do));
-                    nb_seen += __popc(bm);
+                    d32 = warp_max_nn(d32);
                 }
-                __syncwarp();
-                const unsigned mine   = lane < nband ? list[lane] : 0xFFFFFFFFu;
-                const unsigned sorted = warp_sort_u32(mine, lane);
-                d32                   = __uint_as_float(__shfl_sync(kFull, sorted, K - belowk - 1));
-                __syncwarp();
-            }
-
-            // ---- pass 3: certain members and the ambiguous band ----------------
-            float mx_in = 0.0f, my_in = 0.0f;
-            int   n_in = 0, n_amb = 0;
-            float lower = 0.0f, upper = 0.0f;
-            if (!handoff)
-            {
-                lower = __fsub_rd(d32, e2);
-                upper = __fadd_ru(d32, e2);
-                for (int base0 = 0; base0 < m_end; base0 += 32)
+                lower             = __fsub_rd(d32, e2);
+                const float upper = __fadd_ru(d32, e2);
+                int         cin = 0;
+                for (int e0 = 0; e0 < nband; e0 += 32)
                 {
-                    const int m = base0 + lane;
-                    float     sw = 0.0f, Do = 0.0f;
-                    int       j  = 0;
-                    bool      in = false, amb = false;
-                    float     dx = 0.0f, dy = 0.0f;
-                    if (m < m_end)
+                    const int  e   = e0 + lane;
+                    bool       in  = false, amb = false;
+                    if (e < nband)
                     {
-                        elem(m, sw, Do, j);
-                        const float v = fmaxf(sw, Do);
-                        dx            = wx ? sw : Do;
-                        dy            = wx ? Do : sw;
+                        const float v = bv[e];
                         in            = v < lower;
                         amb           = !in && v <= upper;
                         if (in)
                         {
-                            mx_in = fmaxf(mx_in, dx);
-                            my_in = fmaxf(my_in, dy);
+                            mx = fmaxf(mx, bdx[e]);
+                            my = fmaxf(my, bdy[e]);
                         }
                     }
-                    n_in += __popc(__ballot_sync(kFull, in));
+                    cin += in;
                     const unsigned am = __ballot_sync(kFull, amb);
-                    if (amb)
-                    {
-                        const int slot = n_amb + __popc(am & lanemask_lt(lane));
-                        if (slot < 32)
-                        {
-                            list[slot] = (unsigned)j;
-                            ldx[slot]  = dx;
-                            ldy[slot]  = dy;
-                        }
-                    }
+                    const int      sl = n_amb + __popc(am & lanemask_lt(lane));
+                    if (amb && sl < 32)
+                        aj[sl] = (unsigned)e;
                     n_amb += __popc(am);
                 }
-                if (n_amb > 32 || n_amb < 1)
+                n_in += __reduce_add_sync(kFull, cin);
+                if (n_amb > 32 || n_amb < 1 || K - n_in < 1 || K - n_in > n_amb)
+                {
                     handoff = true;
+                    reason  = 4;
+                }
+                __syncwarp();
+            }
+
+            // ---- members whose FP32 marginal is within 2 eps of the members'
+            //      maximum: a superset of those that can hold the FP64 maximum ----
+            int n_cand = 0;
+            if (!handoff)
+            {
+                mx             = warp_max_nn(mx);
+                my             = warp_max_nn(my);
+                const float tx = __fsub_rd(mx, __fmul_ru(2.0f, ea));
+                const float ty = __fsub_rd(my, __fmul_ru(2.0f, eb));
+                for (int b0 = 0; b0 < m_end; b0 += 128)
+                {
+                    const int    m0 = b0 + 4 * lane;
+                    const int    mc = min(m0, p.bufcap - 4);
+                    const float4 a  = *reinterpret_cast<const float4*>(bsw + mc);
+                    const float4 d  = *reinterpret_cast<const float4*>(bdo + mc);
+                    const float  sv[4] = {a.x, a.y, a.z, a.w};
+                    const float  dv[4] = {d.x, d.y, d.z, d.w};
+                    bool         c[4];
+                    bool         anyc = false;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                    {
+                        const float dx = wx ? sv[q] : dv[q], dy = wx ? dv[q] : sv[q];
+                        c[q] = m0 + q < m_end && fmaxf(sv[q], dv[q]) < inlo && (dx >= tx || dy >= ty);
+                        anyc |= c[q];
+                    }
+                    if (__any_sync(kFull, anyc))
+                    {
+                        const uint2 j = *reinterpret_cast<const uint2*>(bj + mc);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                        {
+                            const unsigned cm = __ballot_sync(kFull, c[q]);
+                            const int      sl = n_cand + __popc(cm & lanemask_lt(lane));
+                            if (c[q] && sl < 32)
+                                cj[sl] = u2get16(j, q);
+                            n_cand += __popc(cm);
+                        }
+                    }
+                }
+                for (int e0 = 0; e0 < nband; e0 += 32)
+                {
+                    const int  e = e0 + lane;
+                    const bool c = e < nband && bv[e] < lower && (bdx[e] >= tx || bdy[e] >= ty);
+                    const unsigned cm = __ballot_sync(kFull, c);
+                    const int      sl = n_cand + __popc(cm & lanemask_lt(lane));
+                    if (c && sl < 32)
+                        cj[sl] = bjj[e];
+                    n_cand += __popc(cm);
+                }
+                if (n_cand > 32)
+                {
+                    handoff = true;
+                    reason  = 5;
+                }
                 __syncwarp();
             }
 
             uint32_t out_cnt = 0;
             if (!handoff)
             {
-                mx_in = warp_max((double)mx_in);
-                my_in = warp_max((double)my_in);
-                // ---- pass 4: exact order of the ambiguous band ----------------
-                const double* xa0 = p.X64 + (size_t)a1 * 3 * T;
-                const double* xb0 = p.X64 + (size_t)a2 * 3 * T;
-                const int     ix  = grid.qcell(xa0[i]);
-                const int     iy  = grid.qcell(xb0[i]);
+                // ---- one FP64 round: ambiguous set + max candidates -------------
+                const double qa0 = xa[i], qa1 = xa[T + i], qa2 = xa[2 * T + i];
+                const double qb0 = xb[i], qb1 = xb[T + i], qb2 = xb[2 * T + i];
                 unsigned long long kh = ~0ull, kl = ~0ull;
                 int                slot = lane;
+                double             cx = 0.0, cy = 0.0;
                 if (lane < n_amb)
                 {
-                    const int    j    = (int)list[lane];
-                    const double dx64 = dist3d(p.X64, a1, T, i, j);
-                    const double dy64 = dist3d(p.X64, a2, T, i, j);
-                    l64[lane]         = dx64;
-                    l64[32 + lane]    = dy64;
-                    kh                = dbits(fmax(dx64, dy64));
-                    kl                = grid.rank(ix, iy, xa0[j], xb0[j], j, T);
+                    const int    j  = (int)bjj[aj[lane]];
+                    const double x0 = xa[j], y0 = xb[j];
+                    const double dx = fmax(fmax(fabs(qa0 - x0), fabs(qa1 - xa[T + j])), fabs(qa2 - xa[2 * T + j]));
+                    const double dy = fmax(fmax(fabs(qb0 - y0), fabs(qb1 - xb[T + j])), fabs(qb2 - xb[2 * T + j]));
+                    a64[lane]       = dx;
+                    a64[32 + lane]  = dy;
+                    kh              = dbits(fmax(dx, dy));
+                    kl              = n_amb > 1 ? grid.rank(grid.qcell(qa0), grid.qcell(qb0), x0, y0, j, T) : 0ull;
+                }
+                if (lane < n_cand)
+                {
+                    const int j = (int)cj[lane];
+                    cx = fmax(fmax(fabs(qa0 - xa[j]), fabs(qa1 - xa[T + j])), fabs(qa2 - xa[2 * T + j]));
+                    cy = fmax(fmax(fabs(qb0 - xb[j]), fabs(qb1 - xb[T + j])), fabs(qb2 - xb[2 * T + j]));
                 }
                 __syncwarp();
-                warp_sort_kv(kh, kl, slot, lane);
-                const int need   = K - n_in;
-                if (need < 1 || need > n_amb)
-                    handoff = true; // cannot happen with a valid error bound; stay exact anyway
-                const bool chosen = !handoff && lane < need;
-                float  cx32 = 0.0f, cy32 = 0.0f;
-                double cx64 = 0.0, cy64 = 0.0;
-                if (chosen)
+                if (n_amb > 1)
+                    warp_sort_kv(kh, kl, slot, lane);
+                if (lane < K - n_in)
                 {
-                    cx32 = ldx[slot];
-                    cy32 = ldy[slot];
-                    cx64 = l64[slot];
-                    cy64 = l64[32 + slot];
+                    cx = fmax(cx, a64[slot]);
+                    cy = fmax(cy, a64[32 + slot]);
                 }
-                const float Mx = fmaxf(mx_in, (float)warp_max((double)cx32));
-                const float My = fmaxf(my_in, (float)warp_max((double)cy32));
-                double ex64 = warp_max(cx64), ey64 = warp_max(cy64);
-                // ---- pass 5: certain members that may hold the FP64 maxima -----
-                const float tx = __fsub_rd(Mx, __fmul_ru(2.0f, ea));
-                const float ty = __fsub_rd(My, __fmul_ru(2.0f, eb));
-                for (int base0 = 0; base0 < m_end; base0 += 32)
+                const double ex64 = warp_max_nn(cx), ey64 = warp_max_nn(cy);
+
+                // ---- counts ----------------------------------------------------
+                const double tw = wx ? ex64 : ey64, to = wx ? ey64 : ex64;
+                const float  wlo = __double2float_rd(__dsub_rd(tw, (double)ew));
+                const float  whi = __double2float_ru(__dadd_ru(tw, (double)ew));
+                const float  olo = __double2float_rd(__dsub_rd(to, (double)eo));
+                const float  ohi = __double2float_ru(__dadd_ru(to, (double)eo));
+                // walked marginal: every entry <= whi lies in the walked prefix
+                int w_lo = 0, w_hi = 0;
                 {
-                    const int m = base0 + lane;
-                    if (m < m_end)
+                    int clo = 0, chi = 0;
+                    for (int b0 = 0; b0 < m_end; b0 += 128)
                     {
-                        float sw, Do;
-                        int   j;
-                        elem(m, sw, Do, j);
-                        const float v = fmaxf(sw, Do);
-                        if (v < lower)
+                        const int m0 = b0 + 4 * lane;
+                        if (m0 < m_end)
                         {
-                            const float dx = wx ? sw : Do, dy = wx ? Do : sw;
-                            if (dx >= tx)
-                                ex64 = fmax(ex64, dist3d(p.X64, a1, T, i, j));
-                            if (dy >= ty)
-                                ey64 = fmax(ey64, dist3d(p.X64, a2, T, i, j));
+                            const float4 a = *reinterpret_cast<const float4*>(bsw + m0);
+#pragma unroll
+                            for (int q = 0; q < 4; ++q)
+                            {
+                                const float v = f4get(a, q);
+                                clo += m0 + q < m_end && v < wlo;
+                                chi += m0 + q < m_end && v <= whi;
+                            }
                         }
                     }
+                    w_lo = __reduce_add_sync(kFull, clo);
+                    w_hi = __reduce_add_sync(kFull, chi);
                 }
-                ex64 = warp_max(ex64);
-                ey64 = warp_max(ey64);
-                // ---- counts --------------------------------------------------
-                if (!handoff)
+                // other marginal: chunk from the prefetched probes, then one block
+                int       o_lo, o_hi;
+                const int clo = __popc(__ballot_sync(kFull, probe0 < olo)) + __popc(__ballot_sync(kFull, probe1 < olo));
+                const int chi = __popc(__ballot_sync(kFull, probe0 <= ohi)) + __popc(__ballot_sync(kFull, probe1 <= ohi));
+                if (clo == chi && Llen <= 64 * 64)
                 {
-                    const int nx = count_le_exact(Sa, Pa, Llen, p.X64, a1, T, i, ex64, ea, lane);
-                    const int ny = count_le_exact(Sb, Pb, Llen, p.X64, a2, T, i, ey64, eb, lane);
-                    out_cnt      = (uint32_t)nx | ((uint32_t)ny << 16);
+                    const int   c0 = clo * 64;
+                    const int   e0 = c0 + 2 * lane, e1 = e0 + 1;
+                    const float v0 = e0 < Llen && e0 < c0 + 64 ? So[e0] : inf;
+                    const float v1 = e1 < Llen && e1 < c0 + 64 ? So[e1] : inf;
+                    o_lo = c0 + __reduce_add_sync(kFull, (int)(v0 < olo) + (int)(v1 < olo));
+                    o_hi = c0 + __reduce_add_sync(kFull, (int)(v0 <= ohi) + (int)(v1 <= ohi));
                 }
+                else
+                {
+                    o_lo = warp_rank(So, Llen, olo, true, lane);
+                    o_hi = warp_rank(So, Llen, ohi, false, lane);
+                }
+                // FP64 re-evaluation of both bands in one round
+                const int nbw = w_hi - w_lo, nbo = o_hi - o_lo;
+                int       addw = 0, addo = 0;
+                for (int idx = lane; idx < nbw + nbo; idx += 32)
+                {
+                    if (idx < nbw)
+                    {
+                        const int m = w_lo + idx;
+                        const int j = (int)bj[m];
+                        addw += dist3d(p.X64, wx ? a1 : a2, T, i, j) <= tw;
+                    }
+                    else
+                    {
+                        const int j = (int)Po[o_lo + idx - nbw];
+                        addo += dist3d(p.X64, o, T, i, j) <= to;
+                    }
+                }
+                const int nw = w_lo + __reduce_add_sync(kFull, addw);
+                const int no = o_lo + __reduce_add_sync(kFull, addo);
+                const int nx = wx ? nw : no, ny = wx ? no : nw;
+                out_cnt      = (uint32_t)nx | ((uint32_t)ny << 16);
             }
             if (lane == 0)
             {
@@ -534,6 +872,8 @@ __global__ void __launch_bounds__(kWalkWarps * 32) ksg_walk_kernel(WalkParams p)
                     if (q < p.queue_cap)
                         p.queue[q] = ((unsigned long long)pl << 16) | (unsigned)i;
                     atomicOr(p.status, q < p.queue_cap ? kStatFallback : kStatQueueOverflow);
+                    if (p.reasons)
+                        atomicAdd(p.reasons + reason, 1u);
                 }
                 else
                     p.cnt[(size_t)i * p.pair_count + pl] = out_cnt;
@@ -562,37 +902,45 @@ __global__ void __launch_bounds__(256) ksg_queue_kernel(QueueParams p)
     }
 }
 
-void launch_ksg_x32(const double* X64, int natoms, int T, float4* X32, float* eps_atom, cudaStream_t s)
+cudaError_t launch_ksg_x32(const double* X64, int natoms, int T, float4* X32, float* eps_atom, cudaStream_t s)
 {
     ksg_x32_kernel<<<(natoms * 32 + 255) / 256, 256, 0, s>>>(X64, natoms, T, X32, eps_atom);
+    return cudaGetLastError();
 }
 
-void launch_ksg_rows(const float4* X32, int natoms, int T, int i0, int Q, int Lpad, float* S, uint16_t* P,
-                     cudaStream_t s)
+cudaError_t launch_ksg_rows(const float4* X32, int natoms, int T, int i0, int Q, int Lpad, float* S, uint16_t* P,
+                            cudaStream_t s)
 {
-    int N2 = 1;
+    int N2 = 256;
     while (N2 < T - 1)
         N2 <<= 1;
-    const size_t smem = (size_t)N2 * 8;
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(ksg_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    ksg_rows_kernel<<<(unsigned)((long)natoms * Q), 256, smem, s>>>(X32, T, i0, Q, Lpad, N2, S, P);
+    // bucket pass up to 8192 keys (two key arrays + bins); longer rows use
+    // the bitonic network alone
+    const int    nbin = N2 <= 8192 ? (N2 < 4096 ? N2 : 4096) : 0;
+    const size_t smem = (size_t)N2 * 8 * (nbin ? 2 : 1) + (size_t)nbin * 8;
+    // static shared memory comes on top of the dynamic part: always raise
+    // the limit to what this launch needs
+    cudaFuncSetAttribute(ksg_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ksg_rows_kernel<<<(unsigned)((long)natoms * Q), kRowsThreads, smem, s>>>(X32, T, i0, Q, Lpad, N2, nbin, S, P);
+    return cudaGetLastError();
 }
 
-void launch_ksg_walk(const WalkParams& p, int sms, cudaStream_t s)
+cudaError_t launch_ksg_walk(const WalkParams& p, int sms, cudaStream_t s)
 {
     const size_t smem = (size_t)p.warp_smem * kWalkWarps;
-    cudaFuncSetAttribute(ksg_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(ksg_walk_kernel<kWalkWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ksg_walk_kernel, kWalkWarps * 32, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ksg_walk_kernel<kWalkWarps>, kWalkWarps * 32, smem);
     if (per_sm < 1)
         per_sm = 1;
-    ksg_walk_kernel<<<sms * per_sm, kWalkWarps * 32, smem, s>>>(p);
+    ksg_walk_kernel<kWalkWarps><<<sms * per_sm, kWalkWarps * 32, smem, s>>>(p);
+    return cudaGetLastError();
 }
 
-void launch_ksg_queue(const QueueParams& p, int sms, cudaStream_t s)
+cudaError_t launch_ksg_queue(const QueueParams& p, int sms, cudaStream_t s)
 {
     ksg_queue_kernel<<<sms * 4, 256, 0, s>>>(p);
+    return cudaGetLastError();
 }
 
 } // namespace gc

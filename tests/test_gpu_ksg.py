@@ -83,7 +83,7 @@ def test_fast_path_reference_size(gc):
     torch.cuda.synchronize()
     fast.sync()
     exact.sync()
-    assert fast.handoffs < 0.01 * fast.pairs * T
+    assert fast.handoffs < 0.01 * fast.pairs * T, fast.handoff_reasons
     np.testing.assert_array_equal(out_f.cpu().numpy(), out_e.cpu().numpy())
     fast.close()
     exact.close()
@@ -127,6 +127,8 @@ def test_device_resident_plan(gc, golden, small_x):
         plan.sync()
     assert plan.launches >= 1 and plan.kernel_ms > 0
     assert plan.is_fast
+    # the fast path answers nearly every query itself on smooth data
+    assert plan.handoffs < 0.05 * plan.pairs * T, plan.handoff_reasons
     g = golden["small"]["ksg"]
     want = np.array([g[a1, a2] for a1 in range(1, n) for a2 in range(a1)])  # p = a1(a1-1)/2 + a2
     np.testing.assert_array_equal(out.cpu().numpy(), want)

@@ -61,7 +61,8 @@ class _Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("path", ctypes.c_int), ("pair_begin", ctypes.c_long),
                 ("pair_end", ctypes.c_long), ("stream", ctypes.c_void_p),
                 ("detail_nx", ctypes.POINTER(ctypes.c_int32)),
-                ("detail_ny", ctypes.POINTER(ctypes.c_int32))]
+                ("detail_ny", ctypes.POINTER(ctypes.c_int32)),
+                ("pair_list", ctypes.POINTER(ctypes.c_int64)), ("pair_list_len", ctypes.c_long)]
 
 
 _lib = None
@@ -139,12 +140,16 @@ def _view(x: np.ndarray) -> _TrajView:
     return v
 
 
-def _opts(device=-1, path=PATH_AUTO, pairs=None, stream=None) -> _Opts:
+def _opts(device=-1, path=PATH_AUTO, pairs=None, stream=None, pair_list=None) -> _Opts:
     o = _Opts()
     lib().gc_opts_init(ctypes.byref(o))
     o.device, o.path = device, path
     if pairs is not None:
         o.pair_begin, o.pair_end = int(pairs[0]), int(pairs[1])
+    if pair_list is not None:
+        o._keep = np.ascontiguousarray(pair_list, dtype=np.int64)
+        o.pair_list = o._keep.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        o.pair_list_len = len(o._keep)
     if stream is not None:
         o.stream = ctypes.c_void_p(stream)
     return o
@@ -163,22 +168,24 @@ def gpu_available() -> bool:
 
 
 def kraskov_corrmatrix(x, k: int, *, path: int = PATH_AUTO, device: int = -1, pairs=None,
-                       detail: bool = False):
+                       detail: bool = False, pair_list=None):
     """KSG MI matrix (natoms x natoms), diagonal 2000, as kraskov_corrmatrix.
 
     ``pairs=(begin, end)`` computes only that shard of the pair list
-    p = a1*(a1-1)/2 + a2.  With ``detail=True`` also returns the per-query
-    counts (nx, ny), each of shape (npairs_in_shard, nframes).
+    p = a1*(a1-1)/2 + a2; ``pair_list`` computes exactly the listed pair
+    indices.  With ``detail=True`` also returns the per-query counts
+    (nx, ny), each of shape (npairs_computed, nframes).
     """
     x = _coords(x)
     n, T = x.shape[0], x.shape[1]
     out = np.zeros(n * n)
-    o = _opts(device, path, pairs)
+    o = _opts(device, path, pairs, pair_list=pair_list)
     nx = ny = None
     if detail:
         npairs = n * (n - 1) // 2
         b, e = (0, npairs) if pairs is None else (pairs[0], pairs[1] if pairs[1] > 0 else npairs)
-        nx = np.zeros((max(e - b, 0), T), np.int32)
+        cnt = len(pair_list) if pair_list is not None else max(e - b, 0)
+        nx = np.zeros((cnt, T), np.int32)
         ny = np.zeros_like(nx)
         o.detail_nx = nx.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
         o.detail_ny = ny.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
@@ -282,9 +289,9 @@ class KsgPlan:
     """Device-resident KSG plan: inputs already in HBM, nothing allocated per run."""
 
     def __init__(self, natoms: int, nframes: int, k: int, *, device: int = -1, pairs=None,
-                 path: int = PATH_AUTO):
+                 path: int = PATH_AUTO, pair_list=None):
         self._h = ctypes.c_void_p()
-        o = _opts(device, path, pairs)
+        o = _opts(device, path, pairs, pair_list=pair_list)
         _check(lib().gc_ksg_plan_create(natoms, nframes, k, ctypes.byref(o), ctypes.byref(self._h)))
         self.natoms, self.nframes, self.k = natoms, nframes, k
 

@@ -217,6 +217,7 @@ struct gc_ksg_plan
     DevBuf<double>   X, psi;
     DevBuf<uint32_t> cnt;
     DevBuf<int>      status;
+    DevBuf<int2>     pair_ab; // explicit pair list as (a1, a2), empty for a range
     int              launches = 0;
     cudaEvent_t      ev0 = nullptr, ev1 = nullptr;
     // fast path workspace
@@ -251,7 +252,18 @@ gc_status validate_ksg(int natoms, int T, int k, const gc_opts& o, long* pb, lon
     if (T > 65535)
         return fail(GC_ERR_INVALID, "kraskov_corrmatrix: this build supports at most 65535 frames");
     const long np = (long)natoms * (natoms - 1) / 2;
-    long       b = o.pair_begin, e = o.pair_end <= 0 ? np : o.pair_end;
+    if (o.pair_list)
+    {
+        if (o.pair_list_len < 0)
+            return fail(GC_ERR_INVALID, "negative pair list length");
+        for (long q = 0; q < o.pair_list_len; ++q)
+            if (o.pair_list[q] < 0 || o.pair_list[q] >= np)
+                return fail(GC_ERR_INVALID, "pair list entry out of range");
+        *pb = 0;
+        *pc = o.pair_list_len;
+        return GC_OK;
+    }
+    long b = o.pair_begin, e = o.pair_end <= 0 ? np : o.pair_end;
     if (b < 0 || b > e || e > np)
         return fail(GC_ERR_INVALID, "pair shard out of range");
     *pb = b;
@@ -350,6 +362,18 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
     }
     const std::vector<double> psi = digamma_table(nframes);
     GC_TRY_CUDA(cudaMemcpy(p->psi.p, psi.data(), sizeof(double) * psi.size(), cudaMemcpyHostToDevice));
+    if (o.pair_list && pc > 0)
+    {
+        std::vector<int2> ab((size_t)pc);
+        for (long q = 0; q < pc; ++q)
+        {
+            int a1, a2;
+            gc::pair_from_index((long)o.pair_list[q], &a1, &a2);
+            ab[(size_t)q] = make_int2(a1, a2);
+        }
+        GC_TRY(p->pair_ab.alloc((size_t)pc));
+        GC_TRY_CUDA(cudaMemcpy(p->pair_ab.p, ab.data(), sizeof(int2) * ab.size(), cudaMemcpyHostToDevice));
+    }
     *out = p.release();
     return GC_OK;
 }
@@ -391,6 +415,7 @@ gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi
             w.box = gc::ksg_box_count(T, p->K);
             w.pair_begin = p->pair_begin;
             w.pair_count = p->pair_count;
+            w.pair_ab    = p->pair_ab.p;
             w.shift = p->shift;
             w.nb = p->nb;
             w.bufcap = p->bufcap;
@@ -421,6 +446,7 @@ gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi
             qp.rank_shift = gc::rank_top_shift(w.box, T);
             qp.pair_begin = p->pair_begin;
             qp.pair_count = p->pair_count;
+            qp.pair_ab    = p->pair_ab.p;
             qp.cnt = p->cnt.p;
             qp.queue = p->queue.p;
             qp.queue_len = p->queue_len.p;
@@ -430,7 +456,7 @@ gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi
         }
         else
         {
-            gc::launch_ksg_exact(p->X.p, p->T, p->K, p->pair_begin, p->pair_count, p->cnt.p, s);
+            gc::launch_ksg_exact(p->X.p, p->T, p->K, p->pair_begin, p->pair_count, p->cnt.p, s, p->pair_ab.p);
             p->launches += 1;
         }
         GC_TRY_CUDA(cudaEventRecord(p->ev1, s));
@@ -470,7 +496,7 @@ gc_status gc_ksg_plan_sync(gc_ksg_plan* p)
         // More hand-overs than the queue holds: recompute every query of the
         // shard with the exact kernel (same results, slower).
         cudaStream_t s = p->last_stream;
-        gc::launch_ksg_exact(p->X.p, p->T, p->K, p->pair_begin, p->pair_count, p->cnt.p, s);
+        gc::launch_ksg_exact(p->X.p, p->T, p->K, p->pair_begin, p->pair_count, p->cnt.p, s, p->pair_ab.p);
         gc::launch_ksg_finalize(p->cnt.p, p->pair_count, p->T, p->K, p->psi.p, p->last_mi, s);
         GC_TRY_CUDA(cudaGetLastError());
         GC_TRY_CUDA(cudaStreamSynchronize(s));
@@ -523,6 +549,7 @@ void gc_ksg_plan_destroy(gc_ksg_plan* p)
         p->psi.reset();
         p->cnt.reset();
         p->status.reset();
+        p->pair_ab.reset();
         p->X32.reset();
         p->eps.reset();
         p->S.reset();
@@ -582,7 +609,7 @@ gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, do
     for (long pl = 0; pl < pc; ++pl)
     {
         int a1, a2;
-        gc::pair_from_index(pb + pl, &a1, &a2);
+        gc::pair_from_index(o.pair_list ? (long)o.pair_list[pl] : pb + pl, &a1, &a2);
         mi[(size_t)a1 * n + a2] = pm[(size_t)pl];
         mi[(size_t)a2 * n + a1] = pm[(size_t)pl];
     }
@@ -761,6 +788,7 @@ gc_status gc_ksg_pair(const double* rows6, int nframes, int k, const double* psi
     gc_opts       one = o;
     one.pair_begin = 0;
     one.pair_end   = 0;
+    one.pair_list  = nullptr;
     GC_TRY(validate_ksg(2, T, k, one, &pb, &pc));
     DeviceScope dev(o.device);
     GC_TRY(dev.st);

@@ -29,8 +29,9 @@ void launch_ksg_prepare(const double* xyz, int natoms, int T, double* X, int* st
 
 // Exact FP64 brute-force KSG statistics for pairs [pair_begin, pair_begin+pair_count):
 // writes cnt[i * pair_count + pl] = n_x | n_y << 16 for every query frame i.
+// pair_ab (optional): device (a1, a2) per local pair index of an explicit list.
 void launch_ksg_exact(const double* X, int T, int K, long pair_begin, long pair_count, uint32_t* cnt,
-                      cudaStream_t s);
+                      cudaStream_t s, const int2* pair_ab = nullptr);
 
 // MI per pair from the per-query counts, summed in frame order as mir_xnyn does.
 void launch_ksg_finalize(const uint32_t* cnt, long pair_count, int T, int K, const double* psi,

@@ -74,8 +74,8 @@ constexpr int kExactQBlock = 64;
 } // namespace
 
 __global__ void __launch_bounds__(kExactWarps * 32)
-    ksg_exact_kernel(const double* __restrict__ X, int T, int K, long pair_begin, long pair_count, int nqb,
-                     int rank_shift, uint32_t* __restrict__ cnt)
+    ksg_exact_kernel(const double* __restrict__ X, int T, int K, long pair_begin, long pair_count,
+                     const int2* __restrict__ pair_ab, int nqb, int rank_shift, uint32_t* __restrict__ cnt)
 {
     __shared__ unsigned hist[kExactWarps][256];
     const int  warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -85,7 +85,13 @@ __global__ void __launch_bounds__(kExactWarps * 32)
     if (pl >= pair_count)
         return;
     int a1, a2;
-    pair_from_index(pair_begin + pl, &a1, &a2);
+    if (pair_ab)
+    {
+        a1 = pair_ab[pl].x;
+        a2 = pair_ab[pl].y;
+    }
+    else
+        pair_from_index(pair_begin + pl, &a1, &a2);
     const int box = ksg_box_count(T, K);
     const int i0  = qb * kExactQBlock;
     const int i1  = min(T, i0 + kExactQBlock);
@@ -124,12 +130,12 @@ void launch_ksg_prepare(const double* xyz, int natoms, int T, double* X, int* st
 }
 
 void launch_ksg_exact(const double* X, int T, int K, long pair_begin, long pair_count, uint32_t* cnt,
-                      cudaStream_t s)
+                      cudaStream_t s, const int2* pair_ab)
 {
     const int  nqb   = (T + kExactQBlock - 1) / kExactQBlock;
     const long tasks = pair_count * nqb;
     const int  rank_shift = rank_top_shift(ksg_box_count(T, K), T);
-    ksg_exact_kernel<<<(unsigned)tasks, kExactWarps * 32, 0, s>>>(X, T, K, pair_begin, pair_count, nqb,
+    ksg_exact_kernel<<<(unsigned)tasks, kExactWarps * 32, 0, s>>>(X, T, K, pair_begin, pair_count, pair_ab, nqb,
                                                                   rank_shift, cnt);
 }
 

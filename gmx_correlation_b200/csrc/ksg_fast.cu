@@ -403,18 +403,30 @@ __global__ void __launch_bounds__(WARPS * 32) ksg_walk_kernel(WalkParams p)
         int             iq = (int)(t0 / p.pair_count);
         long            pl = (long)(t0 - (long long)iq * p.pair_count);
         int             a1, a2;
-        pair_from_index(p.pair_begin + pl, &a1, &a2);
+        if (p.pair_ab)
+        {
+            a1 = p.pair_ab[pl].x;
+            a2 = p.pair_ab[pl].y;
+        }
+        else
+            pair_from_index(p.pair_begin + pl, &a1, &a2);
         for (long long t = t0; t < t1; ++t)
         {
             if (t > t0)
             {
-                // advance to the next pair (p = a1*(a1-1)/2 + a2 order)
+                // advance to the next pair (list order, or p = a1*(a1-1)/2 + a2)
                 if (++pl == p.pair_count)
                 {
                     pl = 0;
                     ++iq;
-                    pair_from_index(p.pair_begin, &a1, &a2);
                 }
+                if (p.pair_ab)
+                {
+                    a1 = p.pair_ab[pl].x;
+                    a2 = p.pair_ab[pl].y;
+                }
+                else if (pl == 0)
+                    pair_from_index(p.pair_begin, &a1, &a2);
                 else if (++a2 == a1)
                 {
                     ++a1;
@@ -895,7 +907,13 @@ __global__ void __launch_bounds__(256) ksg_queue_kernel(QueueParams p)
         const long               pl = (long)(q >> 16);
         const int                i  = (int)(q & 0xFFFFu);
         int                      a1, a2;
-        pair_from_index(p.pair_begin + pl, &a1, &a2);
+        if (p.pair_ab)
+        {
+            a1 = p.pair_ab[pl].x;
+            a2 = p.pair_ab[pl].y;
+        }
+        else
+            pair_from_index(p.pair_begin + pl, &a1, &a2);
         const uint32_t c = exact_query(p.X64, p.T, p.K, a1, a2, i, p.box, p.rank_shift, hist[warp], lane);
         if (lane == 0)
             p.cnt[(size_t)i * p.pair_count + pl] = c;

@@ -17,6 +17,7 @@ struct WalkParams
     const uint16_t* P;         // [natoms][Q][Lpad] their frames
     int             Lpad, i0, Q, T, K, box;
     long            pair_begin, pair_count;
+    const int2*     pair_ab;   // optional [pair_count] (a1, a2) of an explicit pair list
     int             shift, nb, bufcap, warp_smem;
     uint32_t*       cnt;        // [T][pair_count] n_x | n_y << 16
     unsigned long long* task_counter;
@@ -34,6 +35,7 @@ struct QueueParams
     const double*       X64;
     int                 T, K, box, rank_shift;
     long                pair_begin, pair_count;
+    const int2*         pair_ab;
     uint32_t*           cnt;
     const unsigned long long* queue;
     const unsigned*     queue_len;

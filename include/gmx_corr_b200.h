@@ -71,6 +71,12 @@ typedef struct gc_opts
      * (x = atom a1, y = atom a2 of pair p, a1 > a2). */
     int32_t* detail_nx;
     int32_t* detail_ny;
+    /* Optional explicit pair list (host array of pair indices
+     * p = a1*(a1-1)/2 + a2): when non-NULL the KSG entry points compute
+     * exactly these pairs, in this order, instead of [pair_begin, pair_end);
+     * detail arrays and plan outputs then follow the list order. */
+    const int64_t* pair_list;
+    long           pair_list_len;
 } gc_opts;
 
 /* Fills *o with the defaults (device -1, GC_PATH_AUTO, all pairs). */

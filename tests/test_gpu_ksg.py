@@ -105,6 +105,25 @@ def test_shard_equals_full(gc, small_x):
     np.testing.assert_array_equal(np.diag(part), 2000.0)
 
 
+def test_pair_list_matches_full_matrix(gc, golden, small_x):
+    g = golden["small"]["ksg"]
+    rng = np.random.default_rng(5)
+    plist = rng.choice(64 * 63 // 2, size=300, replace=False)
+    for path in (0, 1):
+        part, nx, ny = gc.kraskov_corrmatrix(small_x, 10, pair_list=plist, path=path, detail=True)
+        full, fnx, fny = gc.kraskov_corrmatrix(small_x, 10, path=path, detail=True)
+        for q, p in enumerate(plist):
+            a1 = int((1 + np.sqrt(1 + 8 * p)) // 2)
+            while a1 * (a1 - 1) // 2 > p:
+                a1 -= 1
+            while (a1 + 1) * a1 // 2 <= p:
+                a1 += 1
+            a2 = p - a1 * (a1 - 1) // 2
+            assert part[a1, a2] == g[a1, a2] and part[a2, a1] == g[a1, a2]
+            np.testing.assert_array_equal(nx[q], fnx[p])
+            np.testing.assert_array_equal(ny[q], fny[p])
+
+
 def test_prepare_and_wrap_bitwise(gc, oracle, small_x):
     X, psi, scal = gc.kraskov_prepare(small_x)
     Xo, psio = oracle.prepare(small_x)

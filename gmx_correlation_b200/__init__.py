@@ -29,12 +29,19 @@ __all__ = [
     "GCError", "lib", "gpu_available", "kraskov_corrmatrix", "gauss_corrmatrix",
     "gcmi_corrmatrix", "te_matrix", "kraskov_prepare", "kraskov_wrap", "pearsify",
     "write_matrix", "write_xpm_matrix", "read_matrix", "KsgPlan", "PATH_AUTO",
-    "PATH_EXACT_FP64", "LIB_PATH", "probe_fp32",
+    "PATH_EXACT_FP64", "LIB_PATH", "probe_fp32", "screen_features", "ScreenModel", "ksg_screened",
+    "SCREEN_IN", "SCREEN_RAW", "SCREEN_BASE", "SCREEN_COMP",
 ]
 
 LIB_PATH = Path(__file__).resolve().parent / "libgmxcorr_b200.so"
 PATH_AUTO = 0
 PATH_EXACT_FP64 = 1
+# Learned-screen feature layout (include/gmx_corr_b200.h): 23 scalar
+# features, then 17 histogram components (40) or the 64 raw cells (87).
+SCREEN_BASE = 23
+SCREEN_COMP = 17
+SCREEN_IN = SCREEN_BASE + SCREEN_COMP
+SCREEN_RAW = SCREEN_BASE + 64
 
 _STATUS = {
     1: "invalid argument", 2: "no CUDA device", 3: "CUDA error", 4: "zero-variance component",
@@ -63,6 +70,19 @@ class _Opts(ctypes.Structure):
                 ("detail_nx", ctypes.POINTER(ctypes.c_int32)),
                 ("detail_ny", ctypes.POINTER(ctypes.c_int32)),
                 ("pair_list", ctypes.POINTER(ctypes.c_int64)), ("pair_list_len", ctypes.c_long)]
+
+
+class _ScreenOpts(ctypes.Structure):
+    _fields_ = [("audit_frac", ctypes.c_double), ("sigma_max", ctypes.c_double), ("margin", ctypes.c_double),
+                ("seed", ctypes.c_uint64)]
+
+
+class _ScreenReport(ctypes.Structure):
+    _fields_ = [("pairs", ctypes.c_long), ("flagged", ctypes.c_long), ("audited", ctypes.c_long),
+                ("exact", ctypes.c_long), ("audit_accepted", ctypes.c_long), ("threshold", ctypes.c_double),
+                ("audit_max_dr", ctypes.c_double), ("audit_rms_dr", ctypes.c_double),
+                ("final_max_dr", ctypes.c_double), ("ms_features", ctypes.c_float), ("ms_mlp", ctypes.c_float),
+                ("ms_ksg", ctypes.c_float)]
 
 
 _lib = None
@@ -111,6 +131,26 @@ def lib() -> ctypes.CDLL:
                                              ctypes.c_void_p, ctypes.c_void_p]
         L.gc_ksg_plan_destroy.argtypes = [ctypes.c_void_p]
         L.gc_ksg_plan_destroy.restype = None
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.gc_screen_features.argtypes = [ctypes.POINTER(_TrajView), ctypes.c_int, ctypes.POINTER(_Opts), fp, fp, fp]
+        L.gc_screen_model_create.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_void_p)]
+        L.gc_screen_model_destroy.argtypes = [ctypes.c_void_p]
+        L.gc_screen_model_destroy.restype = None
+        L.gc_screen_model_members.argtypes = [ctypes.c_void_p]
+        L.gc_screen_param_stride.restype = ctypes.c_long
+        L.gc_screen_model_get_params.argtypes = [ctypes.c_void_p, fp]
+        L.gc_screen_model_set_params.argtypes = [ctypes.c_void_p, fp]
+        L.gc_screen_model_set_input.argtypes = [ctypes.c_void_p, fp, fp, fp, fp]
+        L.gc_screen_train.argtypes = [ctypes.c_void_p, fp, fp, ctypes.c_long, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_float, ctypes.c_uint64, fp]
+        L.gc_screen_grad.argtypes = [ctypes.c_void_p, fp, fp, ctypes.c_long, fp, fp]
+        L.gc_screen_predict.argtypes = [ctypes.c_void_p, fp, ctypes.c_long, fp]
+        L.gc_screen_opts_init.argtypes = [ctypes.POINTER(_ScreenOpts)]
+        L.gc_screen_opts_init.restype = None
+        L.gc_ksg_screened.argtypes = [ctypes.POINTER(_TrajView), ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.POINTER(_ScreenOpts), ctypes.POINTER(_Opts), dp,
+                                      ctypes.POINTER(_ScreenReport)]
         _ = ip
         _lib = L
     return _lib
@@ -347,3 +387,134 @@ class KsgPlan:
             self.close()
         except Exception:
             pass
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _f32(a, shape=None) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None and a.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {a.shape}")
+    return a
+
+
+def screen_features(x, k: int, *, pca=None, pair_list=None, pairs=None, device: int = -1) -> np.ndarray:
+    """Feature rows of the learned screen for the selected pairs.
+
+    ``pca=(mean[64], comp[17][64])`` gives (npairs, 40) rows; without it the
+    rows hold the 64 raw histogram cells, (npairs, 87).
+    """
+    x = _coords(x)
+    n = x.shape[0]
+    npairs = n * (n - 1) // 2
+    if pair_list is not None:
+        cnt = len(pair_list)
+    elif pairs is not None:
+        cnt = (pairs[1] if pairs[1] > 0 else npairs) - pairs[0]
+    else:
+        cnt = npairs
+    width = SCREEN_IN if pca is not None else SCREEN_RAW
+    out = np.zeros((max(cnt, 0), width), np.float32)
+    o = _opts(device, PATH_AUTO, pairs, pair_list=pair_list)
+    v = _view(x)
+    if pca is not None:
+        pm, pc = _f32(pca[0], (64,)), _f32(pca[1], (SCREEN_COMP, 64))
+        _check(lib().gc_screen_features(ctypes.byref(v), int(k), ctypes.byref(o), _fptr(pm), _fptr(pc), _fptr(out)))
+    else:
+        _check(lib().gc_screen_features(ctypes.byref(v), int(k), ctypes.byref(o), None, None, _fptr(out)))
+    return out
+
+
+class ScreenModel:
+    """Device-resident ensemble of the screen's BF16 networks."""
+
+    def __init__(self, members: int = 4, seed: int = 0, device: int = -1):
+        self._h = ctypes.c_void_p()
+        _check(lib().gc_screen_model_create(int(members), int(seed), int(device), ctypes.byref(self._h)))
+        self.members = members
+        self.stride = int(lib().gc_screen_param_stride())
+        self.sigma_max = 0.0
+        self.margin = 0.0
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros((self.members, self.stride), np.float32)
+        _check(lib().gc_screen_model_get_params(self._h, _fptr(out)))
+        return out
+
+    def set_params(self, params) -> None:
+        p = _f32(params, (self.members, self.stride))
+        _check(lib().gc_screen_model_set_params(self._h, _fptr(p)))
+
+    def set_input(self, feat_mean, feat_sd, pca_mean, pca_comp) -> None:
+        fm, fs = _f32(feat_mean, (SCREEN_IN,)), _f32(feat_sd, (SCREEN_IN,))
+        pm, pc = _f32(pca_mean, (64,)), _f32(pca_comp, (SCREEN_COMP, 64))
+        self._input = (fm, fs, pm, pc)
+        _check(lib().gc_screen_model_set_input(self._h, _fptr(fm), _fptr(fs), _fptr(pm), _fptr(pc)))
+
+    def train(self, feats, target, *, epochs: int = 20, batch: int = 1024, lr: float = 2e-3,
+              seed: int = 0) -> np.ndarray:
+        """Adam on the mean squared error; returns the per-epoch mean loss."""
+        F = _f32(feats)
+        t = _f32(target)
+        if F.ndim != 2 or F.shape[1] != SCREEN_IN or t.shape != (F.shape[0],):
+            raise ValueError("feats must be (n, 40) and target (n,)")
+        loss = np.zeros(epochs, np.float32)
+        _check(lib().gc_screen_train(self._h, _fptr(F), _fptr(t), F.shape[0], int(epochs), int(batch),
+                                     float(lr), int(seed), _fptr(loss)))
+        return loss
+
+    def grad(self, feats, target):
+        """(grad (members, stride), loss (members,)) of one full-batch pass."""
+        F = _f32(feats)
+        t = _f32(target)
+        g = np.zeros((self.members, self.stride), np.float32)
+        loss = np.zeros(self.members, np.float32)
+        _check(lib().gc_screen_grad(self._h, _fptr(F), _fptr(t), F.shape[0], _fptr(g), _fptr(loss)))
+        return g, loss
+
+    def predict(self, feats) -> np.ndarray:
+        """Prediction of every member, shape (members, n)."""
+        F = _f32(feats)
+        out = np.zeros((self.members, F.shape[0]), np.float32)
+        _check(lib().gc_screen_predict(self._h, _fptr(F), F.shape[0], _fptr(out)))
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            lib().gc_screen_model_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ksg_screened(x, k: int, model: ScreenModel, *, audit_frac: float = 0.05, sigma_max=None, margin=None,
+                 seed: int = 12345, device: int = -1, path: int = PATH_AUTO, stream=None):
+    """Screened KSG r(MI) matrix and its report (a dict).
+
+    Exact KSG runs on the pairs whose ensemble spread exceeds ``sigma_max``
+    or whose prediction lies within ``margin`` of the reported threshold,
+    and on a random ``audit_frac`` sample; the rest keep the prediction.
+    ``sigma_max`` / ``margin`` default to the model's calibrated values.
+    """
+    x = _coords(x)
+    n = x.shape[0]
+    so = _ScreenOpts()
+    lib().gc_screen_opts_init(ctypes.byref(so))
+    so.audit_frac = float(audit_frac)
+    so.sigma_max = float(model.sigma_max if sigma_max is None else sigma_max)
+    so.margin = float(model.margin if margin is None else margin)
+    so.seed = int(seed)
+    rep = _ScreenReport()
+    out = np.zeros(n * n)
+    o = _opts(device, path, stream=stream)
+    v = _view(x)
+    _check(lib().gc_ksg_screened(ctypes.byref(v), int(k), model._h, ctypes.byref(so), ctypes.byref(o),
+                                 _dptr(out), ctypes.byref(rep)))
+    report = {f: getattr(rep, f) for f, _ in _ScreenReport._fields_}
+    return out.reshape(n, n), report

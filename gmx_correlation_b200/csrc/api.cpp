@@ -9,6 +9,7 @@
 #include "gc_internal.h"
 #include "gc_geom.h"
 #include "ksg_fast.h"
+#include "host_common.h"
 
 #include <cuda_runtime.h>
 
@@ -23,184 +24,9 @@ namespace {
 
 thread_local std::string g_last_error;
 
-gc_status fail(gc_status st, const std::string& msg)
-{
-    g_last_error = msg;
-    return st;
-}
-
-#define GC_TRY_CUDA(call)                                                                            \
-    do                                                                                               \
-    {                                                                                                \
-        cudaError_t e_ = (call);                                                                     \
-        if (e_ != cudaSuccess)                                                                       \
-            return fail(e_ == cudaErrorMemoryAllocation ? GC_ERR_OUT_OF_MEMORY : GC_ERR_CUDA,         \
-                        std::string(#call) + ": " + cudaGetErrorString(e_));                          \
-    } while (0)
-
-#define GC_TRY(expr)                                                                                 \
-    do                                                                                               \
-    {                                                                                                \
-        gc_status s_ = (expr);                                                                       \
-        if (s_ != GC_OK)                                                                             \
-            return s_;                                                                               \
-    } while (0)
-
-// Switches to the requested device for the lifetime of the guard.
-struct DeviceScope
-{
-    int       prev = -1;
-    gc_status st   = GC_OK;
-    explicit DeviceScope(int dev)
-    {
-        int n = 0;
-        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
-        {
-            cudaGetLastError();
-            st = fail(GC_ERR_NO_DEVICE, "no CUDA device available (this build has no CPU path)");
-            return;
-        }
-        cudaGetDevice(&prev);
-        if (dev >= 0)
-        {
-            if (dev >= n)
-            {
-                st = fail(GC_ERR_INVALID, "device ordinal out of range");
-                return;
-            }
-            if (cudaSetDevice(dev) != cudaSuccess)
-                st = fail(GC_ERR_CUDA, "cudaSetDevice failed");
-        }
-    }
-    ~DeviceScope()
-    {
-        if (prev >= 0)
-            cudaSetDevice(prev);
-    }
-};
-
-template <class T>
-struct DevBuf
-{
-    T*     p = nullptr;
-    size_t n = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    ~DevBuf() { reset(); }
-    void reset()
-    {
-        if (p)
-            cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    gc_status alloc(size_t count)
-    {
-        reset();
-        if (count == 0)
-            count = 1;
-        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-        if (e != cudaSuccess)
-        {
-            cudaGetLastError();
-            p = nullptr;
-            return fail(e == cudaErrorMemoryAllocation ? GC_ERR_OUT_OF_MEMORY : GC_ERR_CUDA,
-                        std::string("cudaMalloc: ") + cudaGetErrorString(e));
-        }
-        n = count;
-        return GC_OK;
-    }
-};
-
-gc_opts defaults()
-{
-    gc_opts o;
-    gc_opts_init(&o);
-    return o;
-}
-
-// digamma table of kraskov_prepare (lib/kraskov.cpp:2217-2219) and
-// digamma_table (lib/transfer_entropy.cpp:41-48): psi[0] = 0,
-// psi[1] = -0.57721566490153, psi[n+1] = psi[n] + 1/n.
-std::vector<double> digamma_table(int N)
-{
-    std::vector<double> psi((size_t)N + 1, 0.0);
-    if (N >= 1)
-        psi[1] = -0.57721566490153;
-    for (int n = 1; n < N; ++n)
-        psi[n + 1] = psi[n] + 1 / (1.0 * n);
-    return psi;
-}
-
-gc_status check_view(const gc_traj_view* v)
-{
-    if (!v)
-        return fail(GC_ERR_INVALID, "null trajectory view");
-    if ((v->xyz == nullptr) == (v->rows == nullptr))
-        return fail(GC_ERR_INVALID, "trajectory view needs exactly one of xyz / rows");
-    if (v->natoms < 0 || v->nframes < 0)
-        return fail(GC_ERR_INVALID, "negative trajectory size");
-    if (v->rows)
-        for (int a = 0; a < v->natoms; ++a)
-            if (!v->rows[a])
-                return fail(GC_ERR_INVALID, "null atom row in trajectory view");
-    return GC_OK;
-}
-
-// Uploads the view's coordinates into a contiguous device block.
-gc_status upload_traj(const gc_traj_view* v, double* d_xyz, cudaStream_t s)
-{
-    const size_t row = (size_t)v->nframes * 3;
-    if (v->xyz)
-    {
-        GC_TRY_CUDA(cudaMemcpyAsync(d_xyz, v->xyz, sizeof(double) * row * v->natoms, cudaMemcpyHostToDevice, s));
-    }
-    else
-    {
-        for (int a = 0; a < v->natoms; ++a)
-            GC_TRY_CUDA(cudaMemcpyAsync(d_xyz + row * a, v->rows[a], sizeof(double) * row, cudaMemcpyHostToDevice, s));
-    }
-    return GC_OK;
-}
-
-gc_status status_to_error(int st)
-{
-    if (st & gc::kStatNonFinite)
-        return fail(GC_ERR_NONFINITE, "non-finite coordinate in the trajectory");
-    if (st & gc::kStatZeroVariance)
-        return fail(GC_ERR_ZERO_VARIANCE,
-                    "a coordinate component has zero variance over the frames (the reference divides by it)");
-    if (st & gc::kStatTimeout)
-        return fail(GC_ERR_TIMEOUT, "a bounded device wait ran out");
-    if (st & gc::kStatInternal)
-        return fail(GC_ERR_INTERNAL, "device-side consistency check failed");
-    return GC_OK;
-}
-
-struct StreamScope
-{
-    cudaStream_t s     = nullptr;
-    bool         owned = false;
-    gc_status    init(void* user)
-    {
-        if (user)
-        {
-            s = (cudaStream_t)user;
-            return GC_OK;
-        }
-        GC_TRY_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-        owned = true;
-        return GC_OK;
-    }
-    ~StreamScope()
-    {
-        if (owned && s)
-            cudaStreamDestroy(s);
-    }
-};
-
 } // namespace
+
+using namespace gc::host;
 
 void gc::set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
 

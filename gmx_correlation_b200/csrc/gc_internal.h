@@ -64,4 +64,79 @@ void launch_blocks(const double* V, int natoms, int T, double* blk, cudaStream_t
 void launch_pair_logdet(const double* blk, int natoms, int T, int mode, double log2pi, double* mat,
                         cudaStream_t s);
 
+// ---- Learned screen --------------------------------------------------------
+constexpr int kScreenStat = 16; // doubles of per-atom statistics
+constexpr int kScreenBase = 23; // scalar features before the histogram part
+constexpr int kScreenHist = 64; // raw 8x8 histogram cells
+constexpr int kScreenComp = 17; // histogram principal components kept
+constexpr int kScreenIn   = kScreenBase + kScreenComp; // 40 network inputs
+
+// Feature rows of pairs [pair_begin, pair_begin + pair_count) (or of the
+// pair_ab list): out[pl][width], width = kScreenIn with a basis pca
+// (mean[64] then comp[ncomp][64]), else kScreenBase + kScreenHist raw.
+// stats: [natoms][kScreenStat] doubles, bins: [natoms][T] bytes (scratch).
+cudaError_t launch_screen_features(const double* xyz, int natoms, int T, int K, long pair_begin, long pair_count,
+                                   const int2* pair_ab, const float* pca, int ncomp, double* stats,
+                                   unsigned char* bins, float* out, int width, cudaStream_t s);
+
+// Network: kScreenIn -> kMlpHidden x 3 (GELU) -> 1, per ensemble member.
+constexpr int  kMlpHidden = 128;
+constexpr long kMlpOffW1  = 0;
+constexpr long kMlpOffB1  = kMlpOffW1 + (long)kMlpHidden * kScreenIn;
+constexpr long kMlpOffW2  = kMlpOffB1 + kMlpHidden;
+constexpr long kMlpOffB2  = kMlpOffW2 + (long)kMlpHidden * kMlpHidden;
+constexpr long kMlpOffW3  = kMlpOffB2 + kMlpHidden;
+constexpr long kMlpOffB3  = kMlpOffW3 + (long)kMlpHidden * kMlpHidden;
+constexpr long kMlpOffW4  = kMlpOffB3 + kMlpHidden;
+constexpr long kMlpOffB4  = kMlpOffW4 + kMlpHidden;
+constexpr long kMlpParams = kMlpOffB4 + 1;
+constexpr long kMlpStride = (kMlpParams + 63) / 64 * 64; // floats per member
+
+// C[z] (+)= A[z] . B[z]^T with A(m,k) = A[z*sAz + m*sAm + k*sAk] and
+// B(n,k) = B[z*sBz + n*sBn + k*sBk]; operands rounded to BF16, FP32
+// accumulation on the tensor cores.  Epilogue: kEpiStore writes (or adds,
+// when accumulate) the product to C[z*sCz + m*ldc + n]; kEpiBias adds
+// bias[z*sbz + n]; kEpiBiasGelu adds the bias, keeps the pre-activation in
+// C and writes GELU of it to H (same layout as C).
+enum
+{
+    kEpiStore    = 0,
+    kEpiBias     = 1,
+    kEpiBiasGelu = 2
+};
+struct MlpGemm
+{
+    const float* A;
+    long         sAz, sAm, sAk;
+    const float* B;
+    long         sBz, sBn, sBk;
+    float*       C;
+    long         sCz, ldc;
+    const float* bias;
+    long         sbz;
+    float*       H;
+    int          M, N, K, Z;
+    int          epi, accumulate;
+};
+cudaError_t launch_mlp_gemm(const MlpGemm& g, cudaStream_t s);
+// X[m][c] = (F[row][c] - mean[c]) / sd[c] with row = idx[base + m] (idx may
+// be null: row = base + m); base = *step * M when step is non-null, else 0.
+cudaError_t launch_mlp_gather(const float* F, const long* idx, const int* step, int M, const float* mean,
+                              const float* sd, float* X, cudaStream_t s);
+// Targets gathered the same way; dY[z][m] = 2 (Y[z][m] - t) / M, and
+// loss[z] += (Y - t)^2 / M.
+cudaError_t launch_mlp_loss(const float* Y, const float* target, const long* idx, const int* step, int M, int Z,
+                            float* dY, float* loss, cudaStream_t s);
+// dZ = dH * GELU'(Zpre), elementwise over n elements.
+cudaError_t launch_mlp_gelu_back(const float* Zpre, float* dH, long n, cudaStream_t s);
+// db[z*sbz + c] = sum over m of dZ[z][m][c] (dZ: [Z][M][N]).
+cudaError_t launch_mlp_colsum(const float* dZ, int M, int N, int Z, float* db, long sbz, cudaStream_t s);
+// Adam over n parameters; hyper = {lr, beta1, beta2, eps}; t = *tstep + 1.
+cudaError_t launch_mlp_adam(float* p, const float* g, float* m, float* v, long n, const float* hyper,
+                            const int* tstep, cudaStream_t s);
+// ++*counter for each pointer that is non-null (one thread).
+cudaError_t launch_mlp_tick(int* a, int* b, cudaStream_t s);
+// Ensemble mean and standard deviation (population) over Z members of Y[z][n].
+cudaError_t launch_mlp_ensemble(const float* Y, long n, int Z, float* mean, float* sd, cudaStream_t s);
+
 } // namespace gc

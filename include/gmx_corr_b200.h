@@ -181,6 +181,98 @@ void gc_ksg_plan_destroy(gc_ksg_plan* plan);
  * denominator. */
 gc_status gc_probe_fp32(int device, double* mix_ops_per_s, double* fma_flops_per_s);
 
+/* ---- Learned KSG screen ----------------------------------------------------
+ * No counterpart in the reference.  An ensemble of small BF16 networks
+ * (GC_SCREEN_IN -> 128 -> 128 -> 128 -> 1, GELU, FP32 accumulation, trained
+ * and evaluated by this library's own kernels) predicts the KSG r(MI) of an
+ * atom pair from cheap per-pair features.  gc_ksg_screened then runs exact
+ * KSG only on the pairs whose prediction is uncertain (ensemble spread) or
+ * close to the reported threshold, plus a seeded random audit sample whose
+ * exact values measure the prediction error.
+ *
+ * Feature row (floats): [0] Gaussian MI of the pair's 6x6 covariance;
+ * [1..6] eigenvalues of the 6x6 joint correlation, descending; [7..12] the
+ * six excess kurtoses (each atom's sorted descending, larger maximum first);
+ * [13..21] |3x3 cross-correlation| sorted descending; [22] k / nframes;
+ * [23..] the 8x8 joint histogram of the atoms' first-principal-axis
+ * projections in rank space (oriented to a non-negative rank correlation,
+ * symmetrised), either projected on GC_SCREEN_COMP principal components or
+ * as the GC_SCREEN_HIST raw cells. */
+#define GC_SCREEN_BASE 23
+#define GC_SCREEN_HIST 64
+#define GC_SCREEN_COMP 17
+#define GC_SCREEN_IN (GC_SCREEN_BASE + GC_SCREEN_COMP) /* 40 */
+#define GC_SCREEN_RAW (GC_SCREEN_BASE + GC_SCREEN_HIST) /* 87 */
+#define GC_SCREEN_HIDDEN 128
+
+typedef struct gc_screen_model gc_screen_model;
+
+/* Features of the pairs opts selects (all pairs, a shard or a list), host
+ * out[pair][GC_SCREEN_IN] projected on the basis pca_mean[64],
+ * pca_comp[GC_SCREEN_COMP][64]; with pca_mean == NULL the raw rows
+ * out[pair][GC_SCREEN_RAW] (used to fit the basis).  nframes <= 16384. */
+gc_status gc_screen_features(const gc_traj_view* traj, int k, const gc_opts* opts, const float* pca_mean,
+                             const float* pca_comp, float* out);
+
+/* An ensemble of `members` networks on `device` (-1 = current), weights
+ * drawn uniform(+-1/sqrt(fan_in)) from `seed`, biases likewise. */
+gc_status gc_screen_model_create(int members, uint64_t seed, int device, gc_screen_model** model);
+void      gc_screen_model_destroy(gc_screen_model* model);
+int       gc_screen_model_members(const gc_screen_model* model);
+/* Floats per member of the parameter block: W1[128][40] b1[128]
+ * W2[128][128] b2[128] W3[128][128] b3[128] W4[1][128] b4[1], then padding. */
+long      gc_screen_param_stride(void);
+/* Host copy of all members' parameters, members * stride floats. */
+gc_status gc_screen_model_get_params(const gc_screen_model* model, float* params);
+gc_status gc_screen_model_set_params(gc_screen_model* model, const float* params);
+/* Standardisation (f - feat_mean) / feat_sd applied to every feature row
+ * before the first layer, and the histogram basis gc_ksg_screened uses
+ * (pca_mean[64], pca_comp[GC_SCREEN_COMP][64]). */
+gc_status gc_screen_model_set_input(gc_screen_model* model, const float* feat_mean, const float* feat_sd,
+                                    const float* pca_mean, const float* pca_comp);
+/* Adam (beta 0.9 / 0.999, eps 1e-8) on the mean squared error of every
+ * member against target[n], over `epochs` passes of shuffled minibatches of
+ * `batch` rows (<= 8192); the learning rate falls from lr to lr / 20 on a
+ * cosine.  feats: host [n][GC_SCREEN_IN].  loss_per_epoch (may be NULL):
+ * mean training loss of each epoch, averaged over members. */
+gc_status gc_screen_train(gc_screen_model* model, const float* feats, const float* target, long n, int epochs,
+                          int batch, float lr, uint64_t seed, float* loss_per_epoch);
+/* One forward and backward pass over all n rows (n <= 8192) with no
+ * update: grad[members * stride] (mean squared error gradient), loss[members]. */
+gc_status gc_screen_grad(gc_screen_model* model, const float* feats, const float* target, long n, float* grad,
+                         float* loss);
+/* Prediction of every member: out[member][n]. */
+gc_status gc_screen_predict(gc_screen_model* model, const float* feats, long n, float* out);
+
+typedef struct gc_screen_opts
+{
+    double   audit_frac; /* random audit sample, fraction of the pairs (0.05) */
+    double   sigma_max;  /* flag a pair when the ensemble's spread exceeds this */
+    double   margin;     /* flag a pair when |r_hat - threshold| < margin */
+    uint64_t seed;       /* audit sample seed */
+} gc_screen_opts;
+
+typedef struct gc_screen_report
+{
+    long   pairs;          /* pairs in the matrix */
+    long   flagged;        /* pairs the screen sent to exact KSG */
+    long   audited;        /* pairs in the random audit sample */
+    long   exact;          /* pairs computed by exact KSG (flagged or audited) */
+    long   audit_accepted; /* audited pairs the screen did not flag */
+    double threshold;      /* reported threshold: mean + 0.5 sd of the positive predicted r */
+    double audit_max_dr;   /* max |r_hat - r_ksg| over audit_accepted pairs */
+    double audit_rms_dr;   /* rms of the same */
+    double final_max_dr;   /* max |r_out - r_ksg| over the audit sample */
+    float  ms_features, ms_mlp, ms_ksg; /* device time of each stage */
+} gc_screen_report;
+
+void gc_screen_opts_init(gc_screen_opts* o);
+/* r(MI) matrix [natoms * natoms] (pearsified, diagonal 1): exact KSG r on
+ * the flagged and audited pairs, the ensemble mean elsewhere.  opts selects
+ * the device, path and stream as for gc_ksg_matrix (pair selection ignored). */
+gc_status gc_ksg_screened(const gc_traj_view* traj, int k, gc_screen_model* model, const gc_screen_opts* sopts,
+                          const gc_opts* opts, double* r, gc_screen_report* report);
+
 /* ---- KSG without device allocation ---------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory (a plugin whose host application owns all device memory through its

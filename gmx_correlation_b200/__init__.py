@@ -359,8 +359,8 @@ class KsgPlan:
     @property
     def handoff_reasons(self) -> dict:
         """Hand-overs of the last run by cause."""
-        names = {1: "walk_longer_than_buffer", 2: "kth_outside_histogram", 3: "band_too_wide",
-                 4: "ambiguous_set_too_large", 5: "too_many_max_candidates"}
+        names = {2: "kth_outside_histogram", 3: "band_too_wide", 4: "ambiguous_set",
+                 5: "maxima_scan_too_long", 6: "count_band_outside_walk"}
         return {v: int(lib().gc_ksg_plan_handoff_reason(self._h, k)) for k, v in names.items()}
 
     @property

@@ -13,6 +13,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -48,17 +49,16 @@ struct gc_ksg_plan
     cudaEvent_t      ev0 = nullptr, ev1 = nullptr;
     // fast path workspace
     bool                         fast = false;
-    int                          Q = 0, Lpad = 0, shift = 0, nb = 0, bufcap = 0;
+    int                          Q = 0, Qp = 0, Lpad = 0, shift = 0;
     DevBuf<float4>               X32;
     DevBuf<float>                eps, S;
     DevBuf<uint16_t>             P;
-    DevBuf<unsigned long long>   task_counter, queue;
-    DevBuf<unsigned>             queue_len;
+    DevBuf<unsigned long long>   task_counter, wres;
+    DevBuf<int>                  pair_order; // task order of the local pairs (atom tiles)
     DevBuf<unsigned long long>   walk_elems;
     DevBuf<unsigned>             reasons;
     long                         reason_counts[8] = {};
     double                       walk_mean = 0.0;
-    unsigned                     queue_cap = 0;
     long                         handoffs = 0;
     const double*                last_xyz = nullptr;
     double*                      last_mi  = nullptr;
@@ -166,23 +166,21 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
     p->fast = o.path != GC_PATH_EXACT_FP64 && nframes - 1 <= 16384 && pc > 0;
     if (p->fast)
     {
-        const int    T    = nframes;
-        p->Lpad           = ((T - 1) + 31) & ~31;
-        const double row  = (double)natoms * p->Lpad * 6.0;
+        const int    T      = nframes;
+        p->Lpad             = ((T - 1) + 31) & ~31;
+        const double row    = (double)natoms * p->Lpad * 6.0;
         const double budget = 8.0 * (1 << 30); // sorted rows of one query block
-        long         q    = (long)(budget / row);
-        p->Q              = (int)(q < 1 ? 1 : (q > T ? T : q));
-        gc::walk_histogram_shape(k, &p->shift, &p->nb);
-        p->bufcap = 640; // walk buffer entries per warp; longer walks go to the exact kernel
+        long         q      = (long)(budget / row) / 32 * 32;
+        q                   = q < 32 ? 32 : q;
+        p->Q                = (int)(q > T ? T : q);
+        p->Qp               = (p->Q + 31) & ~31;
+        p->shift            = gc::walk_histogram_shift(k);
         GC_TRY(p->X32.alloc((size_t)natoms * T));
         GC_TRY(p->eps.alloc((size_t)natoms));
-        GC_TRY(p->S.alloc((size_t)natoms * p->Q * p->Lpad));
-        GC_TRY(p->P.alloc((size_t)natoms * p->Q * p->Lpad));
-        GC_TRY(p->task_counter.alloc(1));
-        const double want = (double)pc * T;
-        p->queue_cap      = (unsigned)(want < 4194304.0 ? want : 4194304.0);
-        GC_TRY(p->queue.alloc(p->queue_cap));
-        GC_TRY(p->queue_len.alloc(1));
+        GC_TRY(p->S.alloc((size_t)natoms * p->Qp * p->Lpad));
+        GC_TRY(p->P.alloc((size_t)natoms * p->Qp * p->Lpad));
+        GC_TRY(p->task_counter.alloc(2));
+        GC_TRY(p->wres.alloc((size_t)p->Q * pc));
         GC_TRY(p->walk_elems.alloc(1));
         GC_TRY(p->reasons.alloc(8));
     }
@@ -199,6 +197,24 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
         }
         GC_TRY(p->pair_ab.alloc((size_t)pc));
         GC_TRY_CUDA(cudaMemcpy(p->pair_ab.p, ab.data(), sizeof(int2) * ab.size(), cudaMemcpyHostToDevice));
+    }
+    if (p->fast && pc > 0)
+    {
+        // Walk tasks visit the pairs tile by tile (16 x 16 atoms), so the
+        // sorted rows of the atoms the running tasks read stay in L2.
+        std::vector<long long> key((size_t)pc);
+        for (long q = 0; q < pc; ++q)
+        {
+            int a1, a2;
+            gc::pair_from_index(o.pair_list ? (long)o.pair_list[q] : pb + q, &a1, &a2);
+            key[(size_t)q] = (((long long)(a1 >> 4) * 65536 + (a2 >> 4)) << 32) | (long long)q;
+        }
+        std::sort(key.begin(), key.end());
+        std::vector<int> order((size_t)pc);
+        for (long q = 0; q < pc; ++q)
+            order[(size_t)q] = (int)(key[(size_t)q] & 0xFFFFFFFFll);
+        GC_TRY(p->pair_order.alloc((size_t)pc));
+        GC_TRY_CUDA(cudaMemcpy(p->pair_order.p, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
     }
     *out = p.release();
     return GC_OK;
@@ -225,59 +241,53 @@ gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi
         {
             const int T = p->T;
             GC_TRY_CUDA(gc::launch_ksg_x32(p->X.p, p->natoms, T, p->X32.p, p->eps.p, s));
-            GC_TRY_CUDA(cudaMemsetAsync(p->queue_len.p, 0, sizeof(unsigned), s));
             GC_TRY_CUDA(cudaMemsetAsync(p->reasons.p, 0, 8 * sizeof(unsigned), s));
             GC_TRY_CUDA(cudaMemsetAsync(p->walk_elems.p, 0, sizeof(unsigned long long), s));
             p->launches += 1;
             gc::WalkParams w{};
-            w.X32 = p->X32.p;
-            w.X64 = p->X.p;
-            w.eps_atom = p->eps.p;
-            w.S = p->S.p;
-            w.P = p->P.p;
-            w.Lpad = p->Lpad;
-            w.T = T;
-            w.K = p->K;
-            w.box = gc::ksg_box_count(T, p->K);
-            w.pair_begin = p->pair_begin;
-            w.pair_count = p->pair_count;
-            w.pair_ab    = p->pair_ab.p;
-            w.shift = p->shift;
-            w.nb = p->nb;
-            w.bufcap = p->bufcap;
-            w.warp_smem = gc::walk_warp_smem(p->nb, p->bufcap);
-            w.cnt = p->cnt.p;
+            w.X32          = p->X32.p;
+            w.X64          = p->X.p;
+            w.eps_atom     = p->eps.p;
+            w.S            = p->S.p;
+            w.P            = p->P.p;
+            w.Lpad         = p->Lpad;
+            w.Qp           = p->Qp;
+            w.T            = T;
+            w.K            = p->K;
+            w.box          = gc::ksg_box_count(T, p->K);
+            w.pair_begin   = p->pair_begin;
+            w.pair_count   = p->pair_count;
+            w.pair_ab      = p->pair_ab.p;
+            w.pair_order   = p->pair_order.p;
+            w.shift        = p->shift;
+            w.wres         = p->wres.p;
+            w.cnt          = p->cnt.p;
             w.task_counter = p->task_counter.p;
-            w.queue = p->queue.p;
-            w.queue_len = p->queue_len.p;
-            w.queue_cap = p->queue_cap;
-            w.status = p->status.p;
-            w.walk_elems = p->walk_elems.p;
-            w.reasons    = p->reasons.p;
+            w.status       = p->status.p;
+            w.walk_elems   = p->walk_elems.p;
+            w.reasons      = p->reasons.p;
             for (int i0 = 0; i0 < T; i0 += p->Q)
             {
                 const int Qb = T - i0 < p->Q ? T - i0 : p->Q;
-                GC_TRY_CUDA(gc::launch_ksg_rows(p->X32.p, p->natoms, T, i0, Qb, p->Lpad, p->S.p, p->P.p, s));
-                GC_TRY_CUDA(cudaMemsetAsync(p->task_counter.p, 0, sizeof(unsigned long long), s));
+                GC_TRY_CUDA(gc::launch_ksg_rows(p->X32.p, p->natoms, T, i0, Qb, p->Qp, p->Lpad, p->S.p, p->P.p, s));
+                GC_TRY_CUDA(cudaMemsetAsync(p->task_counter.p, 0, 2 * sizeof(unsigned long long), s));
                 w.i0 = i0;
                 w.Q  = Qb;
                 GC_TRY_CUDA(gc::launch_ksg_walk(w, p->sms, s));
-                p->launches += 2;
+                GC_TRY_CUDA(gc::launch_ksg_finish(w, p->sms, s));
+                p->launches += 3;
             }
-            gc::QueueParams qp{};
-            qp.X64 = p->X.p;
-            qp.T = T;
-            qp.K = p->K;
-            qp.box = w.box;
-            qp.rank_shift = gc::rank_top_shift(w.box, T);
-            qp.pair_begin = p->pair_begin;
-            qp.pair_count = p->pair_count;
-            qp.pair_ab    = p->pair_ab.p;
-            qp.cnt = p->cnt.p;
-            qp.queue = p->queue.p;
-            qp.queue_len = p->queue_len.p;
-            qp.queue_cap = p->queue_cap;
-            GC_TRY_CUDA(gc::launch_ksg_queue(qp, p->sms, s));
+            gc::FixupParams fp{};
+            fp.X64        = p->X.p;
+            fp.T          = T;
+            fp.K          = p->K;
+            fp.box        = w.box;
+            fp.rank_shift = gc::rank_top_shift(w.box, T);
+            fp.pair_begin = p->pair_begin;
+            fp.pair_count = p->pair_count;
+            fp.pair_ab    = p->pair_ab.p;
+            fp.cnt        = p->cnt.p;
+            GC_TRY_CUDA(gc::launch_ksg_fixup(fp, p->sms, s));
             p->launches += 1;
         }
         else
@@ -306,28 +316,18 @@ gc_status gc_ksg_plan_sync(gc_ksg_plan* p)
     p->handoffs = 0;
     if (p->fast)
     {
-        unsigned h = 0;
-        GC_TRY_CUDA(cudaMemcpy(&h, p->queue_len.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
-        p->handoffs = (long)h;
         unsigned long long we = 0;
         GC_TRY_CUDA(cudaMemcpy(&we, p->walk_elems.p, sizeof(we), cudaMemcpyDeviceToHost));
         p->walk_mean = (double)we / ((double)p->pair_count * p->T);
         unsigned rc[8] = {};
         GC_TRY_CUDA(cudaMemcpy(rc, p->reasons.p, sizeof(rc), cudaMemcpyDeviceToHost));
         for (int r = 0; r < 8; ++r)
+        {
             p->reason_counts[r] = (long)rc[r];
+            p->handoffs += (long)rc[r];
+        }
     }
-    if ((st & gc::kStatQueueOverflow) && p->last_mi && p->pair_count > 0)
-    {
-        // More hand-overs than the queue holds: recompute every query of the
-        // shard with the exact kernel (same results, slower).
-        cudaStream_t s = p->last_stream;
-        gc::launch_ksg_exact(p->X.p, p->T, p->K, p->pair_begin, p->pair_count, p->cnt.p, s, p->pair_ab.p);
-        gc::launch_ksg_finalize(p->cnt.p, p->pair_count, p->T, p->K, p->psi.p, p->last_mi, s);
-        GC_TRY_CUDA(cudaGetLastError());
-        GC_TRY_CUDA(cudaStreamSynchronize(s));
-        st &= ~gc::kStatQueueOverflow;
-    }
+    st &= ~gc::kStatFallback;
     return status_to_error(st);
 }
 
@@ -381,8 +381,6 @@ void gc_ksg_plan_destroy(gc_ksg_plan* p)
         p->S.reset();
         p->P.reset();
         p->task_counter.reset();
-        p->queue.reset();
-        p->queue_len.reset();
         p->walk_elems.reset();
         p->reasons.reset();
     }

@@ -11,21 +11,26 @@
 //                     |d32 - d64| <= eps_a for every marginal distance.
 //   ksg_rows_kernel   per (atom, query): the T-1 marginal distances, sorted
 //                     ascending, with their frame indices (S rows, P rows).
-//   ksg_walk_kernel   per (pair, query), one warp: walks the sorted row of
-//                     the marginal whose k-th distance is larger, gathering
-//                     the other marginal, until the joint k-th distance is
-//                     provably behind; the k-th value comes from a
-//                     shared-memory histogram anchored at the exact lower
-//                     bound max(k-th marginal distances) plus a sorted band.
+//   ksg_walk_kernel   one pair and 32 consecutive queries per warp, one
+//                     query per lane.  Each lane walks the sorted row of the
+//                     marginal whose k-th distance is larger, gathering the
+//                     other marginal, and histograms the joint distances in
+//                     its own shared-memory column (anchored at the exact
+//                     lower bound max(k-th marginal distances)) until the
+//                     joint k-th distance is provably behind.  The bucket of
+//                     the k-th value then bounds a band that two short ranges
+//                     of the two sorted rows enumerate; the members' marginal
+//                     maxima come from backward scans of the same rows.
 //                     Everything within the proven error band 2*eps of a
 //                     decision is re-evaluated in FP64 on the reference's
 //                     normalised coordinates, with the reference's grid-scan
 //                     order deciding exact ties, so n_x and n_y equal the
-//                     reference's counts.  Counts come from warp-parallel
-//                     search in the sorted rows, again with FP64 repair of
-//                     the band around eps_x / eps_y.
-//   ksg_queue_kernel  queries the walk hands over (degenerate histograms,
-//                     oversized tie bands) run through the exact FP64 code.
+//                     reference's counts.  Counts come from binary search in
+//                     the sorted rows, with FP64 repair of the band around
+//                     eps_x / eps_y.
+//   ksg_fixup_kernel  queries a lane hands over (k-th value outside the
+//                     histogram, oversized bands) are marked in the count
+//                     array and recomputed here by the exact FP64 code.
 //
 // Error bound (x32 = fl32(x64 - c), c the component midrange, |x64-c| <= R):
 //   |fl32(x32_i - x32_j) - fl64(x64_i - x64_j)| <= 4 u R (1 + 2^-20),
@@ -89,8 +94,8 @@ __global__ void ksg_x32_kernel(const double* __restrict__ X64, int natoms, int T
 constexpr int kRowsThreads = 256;
 
 __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(const float4* __restrict__ X32, int T, int i0, int Q,
-                                                                int Lpad, int N2, int nbin, float* __restrict__ S,
-                                                                uint16_t* __restrict__ P)
+                                                                int Qp, int Lpad, int N2, int nbin,
+                                                                float* __restrict__ S, uint16_t* __restrict__ P)
 {
     extern __shared__ __align__(16) unsigned char rows_smem[];
     unsigned long long* keys   = reinterpret_cast<unsigned long long*>(rows_smem);      // [N2] sorted output
@@ -235,688 +240,753 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(const float4* __
                 __syncthreads();
             }
     }
-    float*    srow = S + (size_t)row * Lpad;
-    uint16_t* prow = P + (size_t)row * Lpad;
+    // transposed layout: groups of 4 consecutive entries per query, the
+    // queries of a block side by side (see WalkParams)
+    const size_t base    = ((size_t)a * (Lpad >> 2) * Qp + iq) * 4;
+    const size_t gstride = (size_t)Qp * 4;
     for (int m = tid; m < N; m += kRowsThreads)
     {
-        const unsigned long long k = keys[m];
-        srow[m] = __uint_as_float((unsigned)(k >> 32));
-        prow[m] = (uint16_t)(k & 0xFFFFu);
+        const unsigned long long k   = keys[m];
+        const size_t             idx = base + (size_t)(m >> 2) * gstride + (m & 3);
+        S[idx]                       = __uint_as_float((unsigned)(k >> 32));
+        P[idx]                       = (uint16_t)(k & 0xFFFFu);
     }
 }
+
 
 namespace {
 
-// Warp-wide count of sorted row values < t (strict) or <= t.
-__device__ __noinline__ int warp_rank(const float* __restrict__ row, int n, float t, bool strict, int lane)
+// One lane's view of a transposed sorted row (see WalkParams).
+struct LaneRow
 {
-    int lo = 0, hi = n;
-    while (hi - lo > 32)
+    const float*    S;
+    const uint16_t* P;
+    size_t          gstride; // elements between consecutive 4-entry groups
+
+    __device__ __forceinline__ float  s(int m) const { return S[(size_t)(m >> 2) * gstride + (m & 3)]; }
+    __device__ __forceinline__ int    j(int m) const { return P[(size_t)(m >> 2) * gstride + (m & 3)]; }
+    __device__ __forceinline__ float4 s4(int g) const
     {
-        const int  step = (hi - lo + 31) >> 5;
-        const int  p    = lo + lane * step;
-        bool       ok   = false;
-        if (p < hi)
-        {
-            const float v = row[p];
-            ok            = strict ? v < t : v <= t;
-        }
-        const int c = __popc(__ballot_sync(kFull, ok));
-        if (c == 0)
-            hi = lo;
-        else
-        {
-            const int nlo = lo + (c - 1) * step + 1;
-            const int nhi = min(hi, lo + c * step);
-            lo            = nlo;
-            hi            = nhi;
-        }
+        return *reinterpret_cast<const float4*>(S + (size_t)g * gstride);
     }
-    const int p  = lo + lane;
-    bool      ok = false;
-    if (p < hi)
+    __device__ __forceinline__ uint2 j4(int g) const { return *reinterpret_cast<const uint2*>(P + (size_t)g * gstride); }
+};
+
+__device__ __forceinline__ LaneRow lane_row(const WalkParams& p, int atom, int iq)
+{
+    const size_t base = ((size_t)atom * (p.Lpad >> 2) * p.Qp + iq) * 4;
+    return LaneRow{p.S + base, p.P + base, (size_t)p.Qp * 4};
+}
+
+// Four independent binary searches advanced together, so their loads
+// overlap: lo[q] becomes the first position in [lo[q], hi[q]] of row r[q]
+// whose value is not < t[q] (strict[q]) / not <= t[q].
+__device__ __forceinline__ void row_bounds4(const LaneRow (&r)[4], int (&lo)[4], int (&hi)[4], const float (&t)[4],
+                                            const bool (&strict)[4])
+{
+    for (;;)
     {
-        const float v = row[p];
-        ok            = strict ? v < t : v <= t;
-    }
-    return lo + __popc(__ballot_sync(kFull, ok));
-}
-
-__device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
-
-// Warp maximum of non-negative floats / doubles: their IEEE bit patterns
-// order like the values, so single-instruction integer reductions do it.
-__device__ __forceinline__ float warp_max_nn(float v)
-{
-    return __uint_as_float(__reduce_max_sync(kFull, __float_as_uint(v)));
-}
-
-__device__ __forceinline__ double warp_max_nn(double v)
-{
-    const unsigned long long b  = (unsigned long long)__double_as_longlong(v);
-    const unsigned           hi = __reduce_max_sync(kFull, (unsigned)(b >> 32));
-    const unsigned           lo = __reduce_max_sync(kFull, (unsigned)(b >> 32) == hi ? (unsigned)b : 0u);
-    return __longlong_as_double((long long)(((unsigned long long)hi << 32) | lo));
-}
-
-// Bitonic sort of (key_hi, key_lo, payload) per lane, ascending lexicographic.
-__device__ __noinline__ void warp_sort_kv(unsigned long long& kh, unsigned long long& kl, int& pay, int lane)
-{
-#pragma unroll
-    for (int k = 2; k <= 32; k <<= 1)
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1)
-        {
-            const unsigned long long oh = __shfl_xor_sync(kFull, kh, j);
-            const unsigned long long ol = __shfl_xor_sync(kFull, kl, j);
-            const int                op = __shfl_xor_sync(kFull, pay, j);
-            const bool up   = (lane & k) == 0;
-            const bool low  = (lane & j) == 0;
-            const bool less = (oh < kh) || (oh == kh && ol < kl); // other < mine
-            const bool take = (low == up) ? less : !less && !(oh == kh && ol == kl);
-            if (take)
-            {
-                kh  = oh;
-                kl  = ol;
-                pay = op;
-            }
-        }
-}
-
-} // namespace
-
-namespace {
-
-// 4 consecutive sorted-row entries of lane `lane` in the 128-element walk
-// step starting at g0 (m = g0 + 4*lane + q), padded with NaN / frame 0 (a
-// NaN compares false with everything, so padding is never taken).
-__device__ __forceinline__ void load_step(const float* __restrict__ Sw, const uint16_t* __restrict__ Pw, int g0,
-                                          int Llen, int lane, float4& s4, uint2& j2)
-{
-    const int m0 = g0 + 4 * lane;
-    if (m0 + 3 < Llen)
-    {
-        s4 = *reinterpret_cast<const float4*>(Sw + m0);
-        j2 = *reinterpret_cast<const uint2*>(Pw + m0);
-    }
-    else
-    {
-        const float nan = __int_as_float(0x7fc00000);
-        float       v[4];
-        unsigned    j[4];
+        int   mid[4];
+        float v[4];
+        bool  any = false;
 #pragma unroll
         for (int q = 0; q < 4; ++q)
         {
-            v[q] = m0 + q < Llen ? Sw[m0 + q] : nan;
-            j[q] = m0 + q < Llen ? Pw[m0 + q] : 0u;
+            mid[q] = (lo[q] + hi[q]) >> 1;
+            v[q]   = lo[q] < hi[q] ? r[q].s(mid[q]) : 0.0f;
         }
-        s4 = make_float4(v[0], v[1], v[2], v[3]);
-        j2 = make_uint2(j[0] | (j[1] << 16), j[2] | (j[3] << 16));
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (lo[q] < hi[q])
+            {
+                if (strict[q] ? v[q] < t[q] : v[q] <= t[q])
+                    lo[q] = mid[q] + 1;
+                else
+                    hi[q] = mid[q];
+                any |= lo[q] < hi[q];
+            }
+        if (!any)
+            break;
     }
 }
 
-__device__ __forceinline__ float f4get(const float4& v, int q)
+__device__ __forceinline__ double dist3r(const double* __restrict__ r, int T, double q0, double q1, double q2, int j)
 {
-    return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+    return fmax(fmax(fabs(q0 - r[j]), fabs(q1 - r[T + j])), fabs(q2 - r[2 * T + j]));
 }
 
-__device__ __forceinline__ unsigned u2get16(const uint2& v, int q)
+constexpr int kScanCap = 1024; // row entries a backward scan may visit
+constexpr int kAmbCap  = 8;    // ambiguous entries ordered in FP64
+
+// Hand-over causes (WalkParams::reasons index).
+enum
 {
-    return q < 2 ? ((v.x >> (16 * q)) & 0xFFFFu) : ((v.y >> (16 * (q - 2))) & 0xFFFFu);
+    kReasonRange    = 2, // k-th value beyond the histogram's two octaves
+    kReasonBand     = 3, // band larger than kBandCap or inconsistent with the histogram
+    kReasonAmbig    = 4, // ambiguous set inconsistent or larger than kAmbCap
+    kReasonScan     = 5, // backward scan for the maxima exceeded kScanCap
+    kReasonPrefix   = 6  // count band reaches beyond the walked prefix
+};
+
+} // namespace
+
+namespace {
+
+// Per-lane view of one (pair, query): the walked marginal w is the atom with
+// the larger k-th marginal distance L (an exact lower bound of the joint
+// k-th distance), o the other one.
+struct LaneSetup
+{
+    bool          wx; // the walked marginal is x (atom a1)
+    int           w, o;
+    LaneRow       rw, ro;
+    float         L;
+    unsigned      Lb;
+    const float4* X32w;
+    const float4* X32o;
+    float4        xw, xo;
+    float         ew, eo, e2;
+};
+
+// xa / xb: the coordinate rows of a1 / a2 (global memory or the CTA's
+// shared-memory copy).
+__device__ __forceinline__ LaneSetup lane_setup(const WalkParams& p, int a1, int a2, int iql, int i, const float4* xa,
+                                                const float4* xb)
+{
+    LaneSetup     u;
+    const LaneRow ra = lane_row(p, a1, iql), rb = lane_row(p, a2, iql);
+    const float   Ra = ra.s(p.K - 1), Rb = rb.s(p.K - 1);
+    u.wx             = Ra >= Rb;
+    u.w              = u.wx ? a1 : a2;
+    u.o              = u.wx ? a2 : a1;
+    u.rw             = u.wx ? ra : rb;
+    u.ro             = u.wx ? rb : ra;
+    u.L              = u.wx ? Ra : Rb;
+    u.Lb             = __float_as_uint(u.L);
+    u.X32w           = u.wx ? xa : xb;
+    u.X32o           = u.wx ? xb : xa;
+    u.xw             = u.X32w[i];
+    u.xo             = u.X32o[i];
+    const float ea = p.eps_atom[a1], eb = p.eps_atom[a2];
+    u.ew             = u.wx ? ea : eb;
+    u.eo             = u.wx ? eb : ea;
+    u.e2             = __fmul_ru(2.0f, fmaxf(ea, eb));
+    return u;
+}
+
+// CTA task t of a query block: chunk c of (warps per CTA) query groups of 32
+// consecutive queries, one group per warp, for the pair pair_order[k]
+// (pairs in atom-tile order, so the rows the running tasks read stay in L2).
+// Every thread of the CTA calls this; it ends with a barrier.
+struct Task
+{
+    int  c;
+    long pl;
+    int  a1, a2;
+};
+
+__device__ __forceinline__ bool next_task(const WalkParams& p, unsigned long long* counter, long long total,
+                                          long long* s_task, Task& tk)
+{
+    if (threadIdx.x == 0)
+        *s_task = (long long)atomicAdd(counter, 1ull);
+    __syncthreads();
+    const long long t = *s_task;
+    if (t >= total)
+        return false;
+    tk.c         = (int)(t / p.pair_count);
+    const long k = (long)(t - (long long)tk.c * p.pair_count);
+    tk.pl        = p.pair_order ? (long)p.pair_order[k] : k;
+    if (p.pair_ab)
+    {
+        tk.a1 = p.pair_ab[tk.pl].x;
+        tk.a2 = p.pair_ab[tk.pl].y;
+    }
+    else
+        pair_from_index(p.pair_begin + tk.pl, &tk.a1, &tk.a2);
+    return true;
+}
+
+// Copies the coordinate rows of a1 and a2 into shared memory (sx[0, T) and
+// sx[T, 2T)) and returns their addresses; without staging, the global rows.
+__device__ __forceinline__ void pair_rows(const WalkParams& p, int a1, int a2, float4* sx, const float4*& xa,
+                                          const float4*& xb)
+{
+    if (p.staged)
+    {
+        const float4* ga = p.X32 + (size_t)a1 * p.T;
+        const float4* gb = p.X32 + (size_t)a2 * p.T;
+        for (int e = threadIdx.x; e < p.T; e += blockDim.x)
+        {
+            sx[e]       = ga[e];
+            sx[p.T + e] = gb[e];
+        }
+        __syncthreads();
+        xa = sx;
+        xb = sx + p.T;
+    }
+    else
+    {
+        xa = p.X32 + (size_t)a1 * p.T;
+        xb = p.X32 + (size_t)a2 * p.T;
+    }
+}
+
+// Walk result of one (pair, query): bucket of the k-th value, the number of
+// entries below that bucket, the walked length, and a hand-over cause.
+__device__ __forceinline__ unsigned long long pack_walk(int bstar, int prefix, int m_end, int reason)
+{
+    return (unsigned long long)(bstar & 0xFF) | ((unsigned long long)(prefix & 0xFFFF) << 8) |
+           ((unsigned long long)(m_end & 0xFFFF) << 24) | ((unsigned long long)(reason & 0xFF) << 40);
 }
 
 } // namespace
 
-template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) ksg_walk_kernel(WalkParams p)
+// Pass 1: walk the sorted row, histogram v = max(s, d) per lane.
+__global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkParams p)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ long long s_task;
+    const int            warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    float4*              sx   = reinterpret_cast<float4*>(smem_raw);
+    unsigned char*       base = smem_raw + (p.staged ? (size_t)2 * p.T * 16 : 0) + (size_t)warp * kWalkBuckets * 32;
+    // bucket b of this lane: byte b % 4 of word (b / 4) * 32 + lane, so the
+    // 32 lanes of a warp always hit 32 different banks
+    uint8_t* hist = base + lane * 4;
+    auto     H    = [hist](unsigned b) -> uint8_t& { return hist[(b >> 2) * 128 + (b & 3)]; };
+
+    const int       K = p.K, Llen = p.T - 1, shift = p.shift;
+    const int       ngroups = (p.Q + 31) >> 5;
+    const long long total   = (long long)((ngroups + warps - 1) / warps) * p.pair_count;
+    const float     inf     = __int_as_float(0x7f800000);
+    Task            tk;
+    while (next_task(p, p.task_counter, total, &s_task, tk))
+    {
+        const float4* xa;
+        const float4* xb;
+        pair_rows(p, tk.a1, tk.a2, sx, xa, xb);
+        const int       g    = tk.c * warps + warp;
+        const int       iq   = g * 32 + lane;
+        const bool      live = g < ngroups && iq < p.Q;
+        const int       iql  = live ? iq : 0;
+        const LaneSetup u    = lane_setup(p, tk.a1, tk.a2, iql, p.i0 + iql, xa, xb);
+        {
+            uint4* h4 = reinterpret_cast<uint4*>(base);
+            for (int e = lane; e < kWalkBuckets * 32 / 16; e += 32)
+                h4[e] = make_uint4(0u, 0u, 0u, 0u);
+        }
+        __syncwarp();
+        bool saturated = false; // a 255-count bucket below the last one
+
+        // Buckets are 2^shift float ulps above L; v < L counts in cnt_lo.  Every
+        // 16 entries the buckets below the current value are final (later
+        // entries have v >= s), so their running sum R decides the stop value.
+        int    m = 0, cnt_lo = 0, R = 0, thr = 0;
+        float  stop    = inf;
+        bool   walking = live;
+        float4 s4      = u.rw.s4(0);
+        uint2  j4      = u.rw.j4(0);
+        while (walking)
+        {
+            if (m >= Llen) // the whole row walked (m stays a multiple of 4 here)
+                break;
+            float4 ns4 = s4;
+            uint2  nj4 = j4;
+            if (m + 4 < Llen) // prefetch the next group
+            {
+                ns4 = u.rw.s4((m >> 2) + 1);
+                nj4 = u.rw.j4((m >> 2) + 1);
+            }
+            const float    sv[4] = {s4.x, s4.y, s4.z, s4.w};
+            const unsigned jv[4] = {j4.x & 0xFFFFu, j4.x >> 16, j4.y & 0xFFFFu, j4.y >> 16};
+            int            ntk   = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+                if (m + q < Llen && sv[q] <= stop) // taken entries form a prefix
+                {
+                    ++ntk;
+                    const float v = fmaxf(sv[q], dist3f(u.xo, u.X32o[jv[q]]));
+                    if (v < u.L)
+                        ++cnt_lo;
+                    else
+                    {
+                        const unsigned b = min((__float_as_uint(v) - u.Lb) >> shift, (unsigned)kWalkBuckets - 1);
+                        const unsigned h = H(b);
+                        if (h < 255u)
+                            H(b) = (uint8_t)(h + 1u);
+                        else if (b < kWalkBuckets - 1)
+                            saturated = true;
+                    }
+                }
+            }
+            m += ntk;
+            if (ntk < 4)
+                walking = false;
+            else if (stop == inf && (m & 15) == 0)
+            {
+                const float sl = sv[3];
+                const int   bn =
+                    sl >= u.L ? (int)min((__float_as_uint(sl) - u.Lb) >> shift, (unsigned)kWalkBuckets - 1) : 0;
+                for (int b = thr; b < bn; ++b)
+                    R += H(b);
+                thr = max(thr, bn);
+                if (cnt_lo + R >= K)
+                    stop = __fadd_ru(__uint_as_float(u.Lb + ((unsigned)bn << shift)), u.e2);
+            }
+            s4 = ns4;
+            j4 = nj4;
+        }
+        const int m_end = m;
+
+        // bucket of the k-th value
+        if (live)
+        {
+            int bstar, prefix;
+            if (stop != inf)
+            {
+                // cum = #{v < edge(b + 1)} >= K; step down while still >= K
+                int cum = cnt_lo + R, b = thr - 1;
+                while (b > 0 && cum - (int)H(b) >= K)
+                {
+                    cum -= H(b);
+                    --b;
+                }
+                bstar  = b;
+                prefix = cum - H(b);
+            }
+            else
+            {
+                int cum = cnt_lo, b = 0;
+                while (b < kWalkBuckets - 1 && cum + (int)H(b) < K)
+                {
+                    cum += H(b);
+                    ++b;
+                }
+                bstar  = b;
+                prefix = cum;
+            }
+            const int reason = saturated ? kReasonBand : (bstar >= kWalkBuckets - 1 ? kReasonRange : 0);
+            p.wres[(size_t)iq * p.pair_count + tk.pl] = pack_walk(bstar, prefix, m_end, reason);
+        }
+        if (p.walk_elems)
+        {
+            const unsigned we = __reduce_add_sync(kFull, live ? (unsigned)m_end : 0u);
+            if (lane == 0 && we)
+                atomicAdd(p.walk_elems, (unsigned long long)we);
+        }
+        __syncthreads(); // every warp is done with the staged rows and its histogram
+    }
+}
+
+// Pass 2: from the walk's k-th bucket to n_x, n_y (or a hand-over).
+__global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkParams p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int      warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* base = smem_raw + (size_t)warp * p.warp_smem;
-    unsigned*      hist = reinterpret_cast<unsigned*>(base);
-    float*         bsw  = reinterpret_cast<float*>(base + p.nb * 4);
-    float*         bdo  = bsw + p.bufcap;
-    uint16_t*      bj   = reinterpret_cast<uint16_t*>(bdo + p.bufcap);
-    unsigned char* lst  = base + walk_list_offset(p.nb, p.bufcap);
-    float*         bv   = reinterpret_cast<float*>(lst);          // [64] band values
-    unsigned*      bjj  = reinterpret_cast<unsigned*>(lst + 256); // [64] band frames
-    float*         bdx  = reinterpret_cast<float*>(lst + 512);    // [64]
-    float*         bdy  = reinterpret_cast<float*>(lst + 768);    // [64]
-    unsigned*      aj   = reinterpret_cast<unsigned*>(lst + 1024); // [32] ambiguous: band slot
-    unsigned*      cj   = reinterpret_cast<unsigned*>(lst + 1152); // [32] max candidates: frames
-    double*        a64  = reinterpret_cast<double*>(lst + 1280);   // [64] ambiguous dx64 | dy64
+    unsigned char* base = smem_raw + (size_t)warp * kBandSlotBytes * kBandCap * 32;
+    // per-lane columns: band entry e of lane l at [e * 32 + l]: joint value v,
+    // walked-marginal value s, other-marginal value d, row position (>= 0 in
+    // the walked row, -1 - position in the other row) and frame
+    float*    bv = reinterpret_cast<float*>(base) + lane;
+    float*    bs = bv + kBandCap * 32;
+    float*    bd = bs + kBandCap * 32;
+    int*      bp = reinterpret_cast<int*>(bd + kBandCap * 32);
+    uint16_t* bj = reinterpret_cast<uint16_t*>(reinterpret_cast<float*>(base) + 4 * kBandCap * 32) + lane;
 
-    const int       T = p.T, K = p.K, Llen = T - 1;
+    const int       T = p.T, K = p.K, Llen = T - 1, shift = p.shift;
+    const long long total = (long long)((p.Q + 31) >> 5) * p.pair_count;
     const ScanGrid  grid(p.box);
-    const long long total = (long long)p.Q * p.pair_count;
-    const float     inf   = __int_as_float(0x7f800000);
-
     for (;;)
     {
-        long long t0 = 0;
+        // warp task: query group g outer, pairs (in tile order) inner
+        long long t = 0;
         if (lane == 0)
-            t0 = (long long)atomicAdd(p.task_counter, 32ull);
-        t0 = __shfl_sync(kFull, t0, 0);
-        if (t0 >= total)
+            t = (long long)atomicAdd(p.task_counter + 1, 1ull);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= total)
             break;
-        const long long t1 = min(total, t0 + 32);
-        int             iq = (int)(t0 / p.pair_count);
-        long            pl = (long)(t0 - (long long)iq * p.pair_count);
-        int             a1, a2;
+        Task tk;
+        const int  g = (int)(t / p.pair_count);
+        const long k = (long)(t - (long long)g * p.pair_count);
+        tk.pl        = p.pair_order ? (long)p.pair_order[k] : k;
         if (p.pair_ab)
         {
-            a1 = p.pair_ab[pl].x;
-            a2 = p.pair_ab[pl].y;
+            tk.a1 = p.pair_ab[tk.pl].x;
+            tk.a2 = p.pair_ab[tk.pl].y;
         }
         else
-            pair_from_index(p.pair_begin + pl, &a1, &a2);
-        for (long long t = t0; t < t1; ++t)
+            pair_from_index(p.pair_begin + tk.pl, &tk.a1, &tk.a2);
+        const float4* xa   = p.X32 + (size_t)tk.a1 * T;
+        const float4* xb   = p.X32 + (size_t)tk.a2 * T;
+        const int     iq   = g * 32 + lane;
+        const bool    live = iq < p.Q;
+        if (live)
         {
-            if (t > t0)
+            const int                a1 = tk.a1, a2 = tk.a2;
+            const int                i  = p.i0 + iq;
+            const unsigned long long wr = p.wres[(size_t)iq * p.pair_count + tk.pl];
+            const int                bstar = (int)(wr & 0xFF), prefix = (int)((wr >> 8) & 0xFFFF);
+            const int                m_end = (int)((wr >> 24) & 0xFFFF);
+            int                      reason = (int)((wr >> 40) & 0xFF);
+            uint32_t                 out    = kHandOver;
+            const LaneSetup          u      = lane_setup(p, a1, a2, iq, i, xa, xb);
+            const bool     wx = u.wx;
+            const LaneRow& rw = u.rw;
+            const LaneRow& ro = u.ro;
+            const unsigned Lb = u.Lb;
+            const float4*  X32w = u.X32w;
+            const float4*  X32o = u.X32o;
+            const float4   xw = u.xw, xo = u.xo;
+            const float    ew = u.ew, eo = u.eo, e2 = u.e2;
+            if (reason == 0)
             {
-                // advance to the next pair (list order, or p = a1*(a1-1)/2 + a2)
-                if (++pl == p.pair_count)
-                {
-                    pl = 0;
-                    ++iq;
-                }
-                if (p.pair_ab)
-                {
-                    a1 = p.pair_ab[pl].x;
-                    a2 = p.pair_ab[pl].y;
-                }
-                else if (pl == 0)
-                    pair_from_index(p.pair_begin, &a1, &a2);
-                else if (++a2 == a1)
-                {
-                    ++a1;
-                    a2 = 0;
-                }
-            }
-            const int       i  = p.i0 + iq;
-            const float*    Sa = p.S + ((size_t)a1 * p.Q + iq) * p.Lpad;
-            const float*    Sb = p.S + ((size_t)a2 * p.Q + iq) * p.Lpad;
-            const uint16_t* Pa = p.P + ((size_t)a1 * p.Q + iq) * p.Lpad;
-            const uint16_t* Pb = p.P + ((size_t)a2 * p.Q + iq) * p.Lpad;
-            const float     Ra = Sa[K - 1], Rb = Sb[K - 1];
-            const bool      wx = Ra >= Rb; // walk the x (a1) marginal
-            const int       o  = wx ? a2 : a1;
-            const float*    Sw = wx ? Sa : Sb;
-            const uint16_t* Pw = wx ? Pa : Pb;
-            const float*    So = wx ? Sb : Sa;
-            const uint16_t* Po = wx ? Pb : Pa;
-            const float     L  = wx ? Ra : Rb;
-            const unsigned  Lb = __float_as_uint(L);
-            const float4    xo = p.X32[(size_t)o * T + i];
-            const float4*   X32o = p.X32 + (size_t)o * T;
-            const float     ea = p.eps_atom[a1], eb = p.eps_atom[a2];
-            const float     ew = wx ? ea : eb, eo = wx ? eb : ea;
-            const float     e2 = __fmul_ru(2.0f, fmaxf(ea, eb));
-            // probes of the other atom's row for its count (every 64th entry)
-            const int   pr0 = (lane + 1) * 64 - 1, pr1 = (lane + 33) * 64 - 1;
-            const float probe0 = pr0 < Llen ? So[pr0] : inf;
-            const float probe1 = pr1 < Llen ? So[pr1] : inf;
-            bool        handoff = false;
-
-            for (int b = 4 * lane; b < p.nb; b += 128)
-                *reinterpret_cast<uint4*>(hist + b) = make_uint4(0u, 0u, 0u, 0u);
-            __syncwarp();
-
-            // ---- pass 1: walk in 128-entry steps + histogram -------------------
-            // Branch-free step: every lane gathers all four coordinates (padding
-            // entries read frame 0) and the taken mask only gates the counters.
-            int      cnt_lo = 0, R = 0, m_end = 0;
-            unsigned thr  = 0;
-            float    stop = inf;
-            float4   s4;
-            uint2    j2;
-            load_step(Sw, Pw, 0, Llen, lane, s4, j2);
-            for (int g0 = 0; g0 < Llen; g0 += 128)
-            {
-                if (!(__shfl_sync(kFull, s4.x, 0) <= stop))
-                    break;
-                float4 ns4 = make_float4(nanf(""), nanf(""), nanf(""), nanf(""));
-                uint2  nj2 = make_uint2(0u, 0u);
-                if (g0 + 128 < Llen)
-                    load_step(Sw, Pw, g0 + 128, Llen, lane, ns4, nj2);
-                const float4 x0 = X32o[j2.x & 0xFFFFu], x1 = X32o[j2.x >> 16];
-                const float4 x2 = X32o[j2.y & 0xFFFFu], x3 = X32o[j2.y >> 16];
-                const float  d0 = dist3f(xo, x0), d1 = dist3f(xo, x1), d2 = dist3f(xo, x2), d3 = dist3f(xo, x3);
-                const float  sv[4] = {s4.x, s4.y, s4.z, s4.w};
-                const float  dv[4] = {d0, d1, d2, d3};
-                int          nlo = 0, ntk = 0;
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                {
-                    const float    v    = fmaxf(sv[q], dv[q]);
-                    const bool     take = sv[q] <= stop;
-                    const bool     lo   = take && v < L;
-                    const unsigned b    = min((__float_as_uint(v) - Lb) >> p.shift, (unsigned)p.nb - 1);
-                    nlo += lo;
-                    ntk += take;
-                    if (take && !lo)
-                        atomicAdd(&hist[b], 1u);
-                }
-                const int m0 = g0 + 4 * lane;
-                if (m0 < p.bufcap)
-                {
-                    *reinterpret_cast<float4*>(bsw + m0) = s4;
-                    *reinterpret_cast<float4*>(bdo + m0) = make_float4(d0, d1, d2, d3);
-                    *reinterpret_cast<uint2*>(bj + m0)   = j2;
-                }
-                cnt_lo += __reduce_add_sync(kFull, nlo);
-                const int ntake = __reduce_add_sync(kFull, ntk);
-                m_end           = g0 + ntake;
-                __syncwarp();
-                if (stop == inf && ntake > 0)
-                {
-                    const int   last = ntake - 1; // taken entries form a prefix of the step
-                    const float sl   = __shfl_sync(kFull, f4get(s4, last & 3), last >> 2);
-                    if (sl >= L)
+                // ---- band: every entry with inlo <= v <= bandhi, from two row ranges
+                const float elo    = __uint_as_float(Lb + ((unsigned)bstar << shift));
+                const float ehi    = __uint_as_float(Lb + ((unsigned)(bstar + 1) << shift));
+                const float inlo   = __fsub_rd(elo, e2);
+                const float bandhi = __fadd_ru(ehi, e2);
+                if (m_end < Llen && rw.s(m_end) <= bandhi)
+                    reason = kReasonPrefix;
+                const LaneRow rr[4] = {rw, rw, ro, ro};
+                int           lo[4] = {0, 0, 0, 0}, hi[4] = {m_end, m_end, Llen, Llen};
+                const float   tt[4] = {inlo, bandhi, inlo, bandhi};
+                const bool    st[4] = {true, false, true, false};
+                row_bounds4(rr, lo, hi, tt, st);
+                const int mw0 = lo[0], mw1 = lo[1], mo0 = lo[2], mo1 = lo[3];
+                int       nband = 0, nlo = 0;
+                auto add = [&](float v, float sv, float dv, int j, int pos) {
+                    if (nband < kBandCap)
                     {
-                        const unsigned bn  = min((__float_as_uint(sl) - Lb) >> p.shift, (unsigned)p.nb - 1);
-                        int            add = 0;
-                        for (unsigned b = thr + lane; b < bn; b += 32)
-                            add += hist[b];
-                        R += __reduce_add_sync(kFull, add);
-                        thr = bn > thr ? bn : thr;
-                        if (cnt_lo + R >= K)
-                            stop = __fadd_ru(__uint_as_float(Lb + (bn << p.shift)), e2);
+                        bv[nband * 32] = v;
+                        bs[nband * 32] = sv;
+                        bd[nband * 32] = dv;
+                        bp[nband * 32] = pos;
+                        bj[nband * 32] = (uint16_t)j;
                     }
-                }
-                s4 = ns4;
-                j2 = nj2;
-            }
-            if (p.walk_elems && lane == 0)
-                atomicAdd(p.walk_elems, (unsigned long long)m_end);
-            // a walk longer than the buffer goes to the exact kernel (rare)
-            int reason = 0;
-            if (m_end > p.bufcap)
-                reason = 1;
-            handoff = reason != 0;
-
-
-            // ---- bucket of the k-th value: one warp scan over nb/32 buckets/lane
-            int bstar = -1;
-            {
-                const int per = p.nb >> 5; // 2..8 buckets per lane
-                unsigned  c[8];
-                unsigned  own = 0;
-#pragma unroll
-                for (int e = 0; e < 8; ++e)
+                    ++nband;
+                    nlo += v < elo;
+                };
+                // Both ranges in batches of 8: the row loads of a batch, then
+                // its gathers, then the tests, so the loads overlap.
+                for (int m0 = mw0; m0 < mw1; m0 += 8) // s in the band, d <= bandhi
                 {
-                    c[e] = e < per ? hist[lane * per + e] : 0u;
-                    own += c[e];
-                }
-                unsigned incl = own;
+                    int   jj[8];
+                    float sv[8], dv[8];
 #pragma unroll
-                for (int sft = 1; sft < 32; sft <<= 1)
-                {
-                    const unsigned y = __shfl_up_sync(kFull, incl, sft);
-                    if (lane >= sft)
-                        incl += y;
-                }
-                const unsigned need  = (unsigned)(K - cnt_lo);
-                const unsigned excl  = incl - own;
-                const bool     here  = excl < need && need <= incl;
-                int            mine  = -1;
-                if (here)
-                {
-                    unsigned acc = excl;
-#pragma unroll
-                    for (int e = 0; e < 8; ++e)
-                        if (mine < 0 && e < per)
+                    for (int q = 0; q < 8; ++q)
+                        if (m0 + q < mw1)
                         {
-                            acc += c[e];
-                            if (acc >= need)
-                                mine = lane * per + e;
+                            jj[q] = rw.j(m0 + q);
+                            sv[q] = rw.s(m0 + q);
                         }
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        if (m0 + q < mw1)
+                            dv[q] = dist3f(xo, X32o[jj[q]]);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        if (m0 + q < mw1 && dv[q] <= bandhi)
+                            add(fmaxf(sv[q], dv[q]), sv[q], dv[q], jj[q], m0 + q);
                 }
-                const unsigned who = __ballot_sync(kFull, here);
-                bstar              = who ? __shfl_sync(kFull, mine, __ffs(who) - 1) : -1;
-            }
-            if (!handoff && (bstar < 0 || bstar >= p.nb - 1))
-            {
-                handoff = true;
-                reason  = 2;
-            }
-
-            // ---- one pass: certain members, and the band around bucket bstar ----
-            // v < inlo: certainly among the k nearest (d32 >= lower bucket edge);
-            // inlo <= v <= bandhi: the band, which holds the k-th value and every
-            // entry within 2 eps of it; above bandhi: certainly not.
-            const double* xa = p.X64 + (size_t)a1 * 3 * T;
-            const double* xb = p.X64 + (size_t)a2 * 3 * T;
-            float mx = 0.0f, my = 0.0f, inlo = 0.0f, bandhi = 0.0f;
-            int   n_in = 0, nband = 0;
-            if (!handoff)
-            {
-                inlo   = __fsub_rd(__uint_as_float(Lb + ((unsigned)bstar << p.shift)), e2);
-                bandhi = __fadd_ru(__uint_as_float(Lb + ((unsigned)(bstar + 1) << p.shift)), e2);
-                int cin = 0;
-                for (int b0 = 0; b0 < m_end; b0 += 128)
+                for (int m0 = mo0; m0 < mo1; m0 += 8) // d in the band, s < inlo
                 {
-                    const int    m0 = b0 + 4 * lane;
-                    const int    mc = min(m0, p.bufcap - 4);
-                    const float4 a  = *reinterpret_cast<const float4*>(bsw + mc);
-                    const float4 d  = *reinterpret_cast<const float4*>(bdo + mc);
-                    const float  sv[4] = {a.x, a.y, a.z, a.w};
-                    const float  dv[4] = {d.x, d.y, d.z, d.w};
-                    bool         bd[4];
-                    bool         anyb = false;
+                    int   jj[8];
+                    float sv[8], dv[8];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                    {
-                        const float v  = fmaxf(sv[q], dv[q]);
-                        const bool  ok = m0 + q < m_end;
-                        const bool  in = ok && v < inlo;
-                        bd[q]          = ok && !in && v <= bandhi;
-                        anyb |= bd[q];
-                        mx = in ? fmaxf(mx, wx ? sv[q] : dv[q]) : mx;
-                        my = in ? fmaxf(my, wx ? dv[q] : sv[q]) : my;
-                        cin += in;
-                    }
-                    if (__any_sync(kFull, anyb))
-                    {
-                        const uint2 j = *reinterpret_cast<const uint2*>(bj + mc);
-#pragma unroll
-                        for (int q = 0; q < 4; ++q)
+                    for (int q = 0; q < 8; ++q)
+                        if (m0 + q < mo1)
                         {
-                            const unsigned bm = __ballot_sync(kFull, bd[q]);
-                            const int      sl = nband + __popc(bm & lanemask_lt(lane));
-                            if (bd[q] && sl < 64)
-                            {
-                                bv[sl]  = fmaxf(sv[q], dv[q]);
-                                bjj[sl] = u2get16(j, q);
-                                bdx[sl] = wx ? sv[q] : dv[q];
-                                bdy[sl] = wx ? dv[q] : sv[q];
-                            }
-                            nband += __popc(bm);
+                            jj[q] = ro.j(m0 + q);
+                            dv[q] = ro.s(m0 + q);
                         }
-                    }
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        if (m0 + q < mo1)
+                            sv[q] = dist3f(xw, X32w[jj[q]]);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        if (m0 + q < mo1 && sv[q] < inlo)
+                            add(dv[q], sv[q], dv[q], jj[q], -1 - (m0 + q));
                 }
-                n_in = __reduce_add_sync(kFull, cin);
-                if (nband > 64 || K - n_in < 1 || K - n_in > nband)
-                {
-                    handoff = true;
-                    reason  = 3;
-                }
-                __syncwarp();
-            }
+                int       n_in = prefix - nlo; // #{v < inlo}
+                const int r    = K - n_in;     // 1-based rank of the k-th value in the band
+                if (!reason && (nband > kBandCap || r < 1 || r > nband))
+                    reason = kReasonBand;
 
-            // ---- the k-th value from the band, then exact members and the
-            //      ambiguous set (within 2 eps of it) ------------------------------
-            int   n_amb = 0;
-            float lower = 0.0f;
-            if (!handoff)
-            {
-                const int r = K - n_in; // 1-based rank of the k-th value in the band
-                float     d32 = 0.0f;
-                if (nband <= 32)
+                // ---- the k-th FP32 value; certain members and the ambiguous set ---
+                unsigned amb  = 0u;
+                float    lower = 0.0f;
+                int      need  = 0;
+                if (!reason)
                 {
-                    const float mine = lane < nband ? bv[lane] : inf;
-                    int         rk   = 0;
-                    for (int f = 0; f < nband; ++f)
+                    float d32 = 0.0f;
+                    for (int e = 0; e < nband; ++e)
                     {
-                        const float u = __shfl_sync(kFull, mine, f);
-                        rk += u < mine || (u == mine && f < lane);
-                    }
-                    const unsigned hit = __ballot_sync(kFull, lane < nband && rk == r - 1);
-                    d32                = __shfl_sync(kFull, mine, __ffs(hit) - 1);
-                }
-                else
-                {
-                    for (int e = lane; e < nband; e += 32)
-                    {
-                        const float v  = bv[e];
+                        const float v  = bv[e * 32];
                         int         rk = 0;
                         for (int f = 0; f < nband; ++f)
                         {
-                            const float u = bv[f];
+                            const float u = bv[f * 32];
                             rk += u < v || (u == v && f < e);
                         }
                         if (rk == r - 1)
                             d32 = v;
                     }
-                    d32 = warp_max_nn(d32);
-                }
-                lower             = __fsub_rd(d32, e2);
-                const float upper = __fadd_ru(d32, e2);
-                int         cin = 0;
-                for (int e0 = 0; e0 < nband; e0 += 32)
-                {
-                    const int  e   = e0 + lane;
-                    bool       in  = false, amb = false;
-                    if (e < nband)
+                    lower             = __fsub_rd(d32, e2);
+                    const float upper = __fadd_ru(d32, e2);
+                    for (int e = 0; e < nband; ++e)
                     {
-                        const float v = bv[e];
-                        in            = v < lower;
-                        amb           = !in && v <= upper;
-                        if (in)
-                        {
-                            mx = fmaxf(mx, bdx[e]);
-                            my = fmaxf(my, bdy[e]);
-                        }
+                        const float v = bv[e * 32];
+                        if (v < lower)
+                            ++n_in;
+                        else if (v <= upper)
+                            amb |= 1u << e;
                     }
-                    cin += in;
-                    const unsigned am = __ballot_sync(kFull, amb);
-                    const int      sl = n_amb + __popc(am & lanemask_lt(lane));
-                    if (amb && sl < 32)
-                        aj[sl] = (unsigned)e;
-                    n_amb += __popc(am);
+                    need = K - n_in;
+                    if (need < 1 || need > __popc(amb))
+                        reason = kReasonAmbig;
                 }
-                n_in += __reduce_add_sync(kFull, cin);
-                if (n_amb > 32 || n_amb < 1 || K - n_in < 1 || K - n_in > n_amb)
-                {
-                    handoff = true;
-                    reason  = 4;
-                }
-                __syncwarp();
-            }
 
-            // ---- members whose FP32 marginal is within 2 eps of the members'
-            //      maximum: a superset of those that can hold the FP64 maximum ----
-            int n_cand = 0;
-            if (!handoff)
-            {
-                mx             = warp_max_nn(mx);
-                my             = warp_max_nn(my);
-                const float tx = __fsub_rd(mx, __fmul_ru(2.0f, ea));
-                const float ty = __fsub_rd(my, __fmul_ru(2.0f, eb));
-                for (int b0 = 0; b0 < m_end; b0 += 128)
+                // ---- marginal maxima over the members, then the counts -----------
+                // Fast path: when no other member lies within 2 eps below the
+                // FP32 maximum member of a marginal, that member holds the FP64
+                // maximum; when no other row entry lies within 2 eps of it
+                // either, its row position gives the count.  Otherwise every
+                // member within 2 eps gets an FP64 look and an FP64-repaired
+                // binary search counts.
+                const double* xa64 = p.X64 + (size_t)a1 * 3 * T;
+                const double* xb64 = p.X64 + (size_t)a2 * 3 * T;
+                const double* xw64 = wx ? xa64 : xb64;
+                const double* xo64 = wx ? xb64 : xa64;
+                unsigned      amem = 0u; // ambiguous band entries that are members
+                if (!reason)
                 {
-                    const int    m0 = b0 + 4 * lane;
-                    const int    mc = min(m0, p.bufcap - 4);
-                    const float4 a  = *reinterpret_cast<const float4*>(bsw + mc);
-                    const float4 d  = *reinterpret_cast<const float4*>(bdo + mc);
-                    const float  sv[4] = {a.x, a.y, a.z, a.w};
-                    const float  dv[4] = {d.x, d.y, d.z, d.w};
-                    bool         c[4];
-                    bool         anyc = false;
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                    {
-                        const float dx = wx ? sv[q] : dv[q], dy = wx ? dv[q] : sv[q];
-                        c[q] = m0 + q < m_end && fmaxf(sv[q], dv[q]) < inlo && (dx >= tx || dy >= ty);
-                        anyc |= c[q];
-                    }
-                    if (__any_sync(kFull, anyc))
-                    {
-                        const uint2 j = *reinterpret_cast<const uint2*>(bj + mc);
-#pragma unroll
-                        for (int q = 0; q < 4; ++q)
-                        {
-                            const unsigned cm = __ballot_sync(kFull, c[q]);
-                            const int      sl = n_cand + __popc(cm & lanemask_lt(lane));
-                            if (c[q] && sl < 32)
-                                cj[sl] = u2get16(j, q);
-                            n_cand += __popc(cm);
-                        }
-                    }
-                }
-                for (int e0 = 0; e0 < nband; e0 += 32)
-                {
-                    const int  e = e0 + lane;
-                    const bool c = e < nband && bv[e] < lower && (bdx[e] >= tx || bdy[e] >= ty);
-                    const unsigned cm = __ballot_sync(kFull, c);
-                    const int      sl = n_cand + __popc(cm & lanemask_lt(lane));
-                    if (c && sl < 32)
-                        cj[sl] = bjj[e];
-                    n_cand += __popc(cm);
-                }
-                if (n_cand > 32)
-                {
-                    handoff = true;
-                    reason  = 5;
-                }
-                __syncwarp();
-            }
-
-            uint32_t out_cnt = 0;
-            if (!handoff)
-            {
-                // ---- one FP64 round: ambiguous set + max candidates -------------
-                const double qa0 = xa[i], qa1 = xa[T + i], qa2 = xa[2 * T + i];
-                const double qb0 = xb[i], qb1 = xb[T + i], qb2 = xb[2 * T + i];
-                unsigned long long kh = ~0ull, kl = ~0ull;
-                int                slot = lane;
-                double             cx = 0.0, cy = 0.0;
-                if (lane < n_amb)
-                {
-                    const int    j  = (int)bjj[aj[lane]];
-                    const double x0 = xa[j], y0 = xb[j];
-                    const double dx = fmax(fmax(fabs(qa0 - x0), fabs(qa1 - xa[T + j])), fabs(qa2 - xa[2 * T + j]));
-                    const double dy = fmax(fmax(fabs(qb0 - y0), fabs(qb1 - xb[T + j])), fabs(qb2 - xb[2 * T + j]));
-                    a64[lane]       = dx;
-                    a64[32 + lane]  = dy;
-                    kh              = dbits(fmax(dx, dy));
-                    kl              = n_amb > 1 ? grid.rank(grid.qcell(qa0), grid.qcell(qb0), x0, y0, j, T) : 0ull;
-                }
-                if (lane < n_cand)
-                {
-                    const int j = (int)cj[lane];
-                    cx = fmax(fmax(fabs(qa0 - xa[j]), fabs(qa1 - xa[T + j])), fabs(qa2 - xa[2 * T + j]));
-                    cy = fmax(fmax(fabs(qb0 - xb[j]), fabs(qb1 - xb[T + j])), fabs(qb2 - xb[2 * T + j]));
-                }
-                __syncwarp();
-                if (n_amb > 1)
-                    warp_sort_kv(kh, kl, slot, lane);
-                if (lane < K - n_in)
-                {
-                    cx = fmax(cx, a64[slot]);
-                    cy = fmax(cy, a64[32 + slot]);
-                }
-                const double ex64 = warp_max_nn(cx), ey64 = warp_max_nn(cy);
-
-                // ---- counts ----------------------------------------------------
-                const double tw = wx ? ex64 : ey64, to = wx ? ey64 : ex64;
-                const float  wlo = __double2float_rd(__dsub_rd(tw, (double)ew));
-                const float  whi = __double2float_ru(__dadd_ru(tw, (double)ew));
-                const float  olo = __double2float_rd(__dsub_rd(to, (double)eo));
-                const float  ohi = __double2float_ru(__dadd_ru(to, (double)eo));
-                // walked marginal: every entry <= whi lies in the walked prefix
-                int w_lo = 0, w_hi = 0;
-                {
-                    int clo = 0, chi = 0;
-                    for (int b0 = 0; b0 < m_end; b0 += 128)
-                    {
-                        const int m0 = b0 + 4 * lane;
-                        if (m0 < m_end)
-                        {
-                            const float4 a = *reinterpret_cast<const float4*>(bsw + m0);
-#pragma unroll
-                            for (int q = 0; q < 4; ++q)
-                            {
-                                const float v = f4get(a, q);
-                                clo += m0 + q < m_end && v < wlo;
-                                chi += m0 + q < m_end && v <= whi;
-                            }
-                        }
-                    }
-                    w_lo = __reduce_add_sync(kFull, clo);
-                    w_hi = __reduce_add_sync(kFull, chi);
-                }
-                // other marginal: chunk from the prefetched probes, then one block
-                int       o_lo, o_hi;
-                const int clo = __popc(__ballot_sync(kFull, probe0 < olo)) + __popc(__ballot_sync(kFull, probe1 < olo));
-                const int chi = __popc(__ballot_sync(kFull, probe0 <= ohi)) + __popc(__ballot_sync(kFull, probe1 <= ohi));
-                if (clo == chi && Llen <= 64 * 64)
-                {
-                    const int   c0 = clo * 64;
-                    const int   e0 = c0 + 2 * lane, e1 = e0 + 1;
-                    const float v0 = e0 < Llen && e0 < c0 + 64 ? So[e0] : inf;
-                    const float v1 = e1 < Llen && e1 < c0 + 64 ? So[e1] : inf;
-                    o_lo = c0 + __reduce_add_sync(kFull, (int)(v0 < olo) + (int)(v1 < olo));
-                    o_hi = c0 + __reduce_add_sync(kFull, (int)(v0 <= ohi) + (int)(v1 <= ohi));
-                }
-                else
-                {
-                    o_lo = warp_rank(So, Llen, olo, true, lane);
-                    o_hi = warp_rank(So, Llen, ohi, false, lane);
-                }
-                // FP64 re-evaluation of both bands in one round
-                const int nbw = w_hi - w_lo, nbo = o_hi - o_lo;
-                int       addw = 0, addo = 0;
-                for (int idx = lane; idx < nbw + nbo; idx += 32)
-                {
-                    if (idx < nbw)
-                    {
-                        const int m = w_lo + idx;
-                        const int j = (int)bj[m];
-                        addw += dist3d(p.X64, wx ? a1 : a2, T, i, j) <= tw;
-                    }
+                    const int n_amb = __popc(amb);
+                    if (n_amb == need)
+                        amem = amb;
+                    else if (n_amb > kAmbCap)
+                        reason = kReasonAmbig;
                     else
                     {
-                        const int j = (int)Po[o_lo + idx - nbw];
-                        addo += dist3d(p.X64, o, T, i, j) <= to;
+                        // order the ambiguous entries by (FP64 joint distance, scan rank)
+                        unsigned long long kh[kAmbCap], kl[kAmbCap];
+                        int                slot[kAmbCap];
+                        const double       qw0 = xw64[i], qw1 = xw64[T + i], qw2 = xw64[2 * T + i];
+                        const double       qo0 = xo64[i], qo1 = xo64[T + i], qo2 = xo64[2 * T + i];
+                        const int          ix = grid.qcell(xa64[i]), iy = grid.qcell(xb64[i]);
+                        int                c  = 0;
+                        for (unsigned am = amb; am; am &= am - 1, ++c)
+                        {
+                            const int    e  = __ffs(am) - 1;
+                            const int    j  = bj[e * 32];
+                            const double dw = dist3r(xw64, T, qw0, qw1, qw2, j);
+                            const double dq = dist3r(xo64, T, qo0, qo1, qo2, j);
+                            slot[c]         = e;
+                            kh[c]           = dbits(fmax(dw, dq));
+                            kl[c]           = grid.rank(ix, iy, xa64[j], xb64[j], j, T);
+                        }
+                        for (int x = 0; x < n_amb; ++x)
+                        {
+                            int rk = 0;
+                            for (int y = 0; y < n_amb; ++y)
+                                rk += kh[y] < kh[x] || (kh[y] == kh[x] && kl[y] < kl[x]);
+                            if (rk < need)
+                                amem |= 1u << slot[x];
+                        }
                     }
                 }
-                const int nw = w_lo + __reduce_add_sync(kFull, addw);
-                const int no = o_lo + __reduce_add_sync(kFull, addo);
-                const int nx = wx ? nw : no, ny = wx ? no : nw;
-                out_cnt      = (uint32_t)nx | ((uint32_t)ny << 16);
-            }
-            if (lane == 0)
-            {
-                if (handoff)
+                int ncount[2] = {0, 0}; // counts of the walked and the other marginal
+                int steps     = 0;
+                for (int side = 0; side < 2 && !reason; ++side)
                 {
-                    const unsigned q = atomicAdd(p.queue_len, 1u);
-                    if (q < p.queue_cap)
-                        p.queue[q] = ((unsigned long long)pl << 16) | (unsigned)i;
-                    atomicOr(p.status, q < p.queue_cap ? kStatFallback : kStatQueueOverflow);
-                    if (p.reasons)
-                        atomicAdd(p.reasons + reason, 1u);
+                    const LaneRow& row  = side == 0 ? rw : ro;
+                    const float4*  Xc   = side == 0 ? X32o : X32w; // membership: the other marginal < inlo
+                    const float4   xc   = side == 0 ? xo : xw;
+                    const double*  x64  = side == 0 ? xw64 : xo64;
+                    const float    eps  = side == 0 ? ew : eo;
+                    const float*   bval = side == 0 ? bs : bd;
+                    // band members
+                    float top = -1.0f, sec = -1.0f;
+                    int   ptop = -1;
+                    for (int e = 0; e < nband; ++e)
+                    {
+                        if (!(bv[e * 32] < lower || ((amem >> e) & 1u)))
+                            continue;
+                        const float val  = bval[e * 32];
+                        const int   pos  = bp[e * 32];
+                        const int   prow = side == 0 ? (pos >= 0 ? pos : -1) : (pos < 0 ? -1 - pos : -1);
+                        if (val > top)
+                        {
+                            sec  = top;
+                            top  = val;
+                            ptop = prow;
+                        }
+                        else if (val > sec)
+                            sec = val;
+                    }
+                    // members with v < inlo: the first one below the band start
+                    // in this row holds their maximum (four entries per round)
+                    int   mm = (side == 0 ? mw0 : mo0) - 1, first = -1;
+                    float fval = -1.0f, fsec = -1.0f;
+                    while (mm >= 0 && first < 0)
+                    {
+                        int   jj[4];
+                        float sv[4];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            if (mm - q >= 0)
+                            {
+                                jj[q] = row.j(mm - q);
+                                sv[q] = row.s(mm - q);
+                            }
+                        bool ok[4];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            ok[q] = mm - q >= 0 && dist3f(xc, Xc[jj[q]]) < inlo;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            if (ok[q])
+                            {
+                                if (first < 0)
+                                {
+                                    first = mm - q;
+                                    fval  = sv[q];
+                                }
+                                else
+                                    fsec = fmaxf(fsec, sv[q]);
+                            }
+                        mm -= 4; // the next unexamined position
+                        steps += 4;
+                        if (first < 0 && steps > kScanCap)
+                            reason = kReasonScan;
+                    }
+                    if (reason)
+                        break;
+                    if (first >= 0)
+                    {
+                        if (fval > top)
+                        {
+                            sec  = fmaxf(sec, top);
+                            top  = fval;
+                            ptop = first;
+                        }
+                        else
+                            sec = fmaxf(sec, fval);
+                        sec = fmaxf(sec, fsec);
+                    }
+                    const float tie = __fsub_rd(top, __fmul_ru(2.0f, eps));
+                    const float chi = __fadd_ru(top, __fmul_ru(2.0f, eps));
+                    // members below the examined entries that are still within 2 eps
+                    for (; first >= 0 && mm >= 0; --mm)
+                    {
+                        const float sv = row.s(mm);
+                        if (sv < tie)
+                            break;
+                        if (++steps > kScanCap)
+                        {
+                            reason = kReasonScan;
+                            break;
+                        }
+                        if (dist3f(xc, Xc[row.j(mm)]) < inlo)
+                            sec = fmaxf(sec, sv);
+                    }
+                    if (reason)
+                        break;
+                    bool fast = ptop >= 0 && sec < tie;
+                    if (fast && ptop > 0 && row.s(ptop - 1) >= tie)
+                        fast = false;
+                    if (fast && ptop + 1 < Llen && row.s(ptop + 1) <= chi)
+                        fast = false;
+                    if (fast)
+                    {
+                        ncount[side] = ptop + 1;
+                        continue;
+                    }
+                    // FP64 maximum over every member within 2 eps of top
+                    const double q0 = x64[i], q1 = x64[T + i], q2 = x64[2 * T + i];
+                    double       best = -1.0;
+                    for (int e = 0; e < nband; ++e)
+                        if ((bv[e * 32] < lower || ((amem >> e) & 1u)) && bval[e * 32] >= tie)
+                            best = fmax(best, dist3r(x64, T, q0, q1, q2, bj[e * 32]));
+                    for (int pos = first; pos >= 0; --pos)
+                    {
+                        const float sv = row.s(pos);
+                        if (sv < tie)
+                            break;
+                        if (++steps > kScanCap)
+                        {
+                            reason = kReasonScan;
+                            break;
+                        }
+                        const int j = row.j(pos);
+                        if (dist3f(xc, Xc[j]) < inlo)
+                            best = fmax(best, dist3r(x64, T, q0, q1, q2, j));
+                    }
+                    if (reason)
+                        break;
+                    // count: every entry below the FP64 band, plus the band in FP64
+                    const float   tlo   = __double2float_rd(__dsub_rd(best, (double)eps));
+                    const float   thi   = __double2float_ru(__dadd_ru(best, (double)eps));
+                    const LaneRow rr[4] = {row, row, row, row};
+                    int           lo[4] = {0, 0, 0, 0}, hi[4] = {Llen, Llen, 0, 0};
+                    const float   tt[4] = {tlo, thi, 0.0f, 0.0f};
+                    const bool    st[4] = {true, false, true, true};
+                    row_bounds4(rr, lo, hi, tt, st);
+                    int n = lo[0];
+                    for (int pos = lo[0]; pos < lo[1]; ++pos)
+                        n += dist3r(x64, T, q0, q1, q2, row.j(pos)) <= best;
+                    ncount[side] = n;
                 }
-                else
-                    p.cnt[(size_t)i * p.pair_count + pl] = out_cnt;
+                if (!reason)
+                {
+                    const int nx = wx ? ncount[0] : ncount[1], ny = wx ? ncount[1] : ncount[0];
+                    out          = (uint32_t)nx | ((uint32_t)ny << 16);
+                }
             }
-            __syncwarp();
+            if (reason)
+            {
+                out = kHandOver;
+                atomicOr(p.status, kStatFallback);
+                if (p.reasons)
+                    atomicAdd(p.reasons + reason, 1u);
+            }
+            p.cnt[(size_t)i * p.pair_count + tk.pl] = out;
         }
+        __syncwarp(); // band columns of every lane are free for the next task
     }
 }
 
-// Exact FP64 statistics for the queries the walk handed over.
-__global__ void __launch_bounds__(256) ksg_queue_kernel(QueueParams p)
+// Exact FP64 statistics for the queries the walk marked with kHandOver.
+__global__ void __launch_bounds__(256) ksg_fixup_kernel(FixupParams p)
 {
     __shared__ unsigned hist[8][256];
-    const int      warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const unsigned n    = min(*p.queue_len, p.queue_cap);
-    for (unsigned e = blockIdx.x * 8 + warp; e < n; e += gridDim.x * 8)
+    const int       warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long n    = (long long)p.T * p.pair_count;
+    for (long long c0 = ((long long)blockIdx.x * 8 + warp) * 32; c0 < n; c0 += (long long)gridDim.x * 8 * 32)
     {
-        const unsigned long long q  = p.queue[e];
-        const long               pl = (long)(q >> 16);
-        const int                i  = (int)(q & 0xFFFFu);
-        int                      a1, a2;
-        if (p.pair_ab)
+        const long long e  = c0 + lane;
+        unsigned        hm = __ballot_sync(kFull, e < n && p.cnt[e] == kHandOver);
+        while (hm)
         {
-            a1 = p.pair_ab[pl].x;
-            a2 = p.pair_ab[pl].y;
+            const int       src = __ffs(hm) - 1;
+            const long long idx = c0 + src;
+            hm &= hm - 1;
+            const int  i  = (int)(idx / p.pair_count);
+            const long pl = (long)(idx - (long long)i * p.pair_count);
+            int        a1, a2;
+            if (p.pair_ab)
+            {
+                a1 = p.pair_ab[pl].x;
+                a2 = p.pair_ab[pl].y;
+            }
+            else
+                pair_from_index(p.pair_begin + pl, &a1, &a2);
+            const uint32_t c = exact_query(p.X64, p.T, p.K, a1, a2, i, p.box, p.rank_shift, hist[warp], lane);
+            if (lane == 0)
+                p.cnt[idx] = c;
+            __syncwarp();
         }
-        else
-            pair_from_index(p.pair_begin + pl, &a1, &a2);
-        const uint32_t c = exact_query(p.X64, p.T, p.K, a1, a2, i, p.box, p.rank_shift, hist[warp], lane);
-        if (lane == 0)
-            p.cnt[(size_t)i * p.pair_count + pl] = c;
     }
 }
 
@@ -926,8 +996,8 @@ cudaError_t launch_ksg_x32(const double* X64, int natoms, int T, float4* X32, fl
     return cudaGetLastError();
 }
 
-cudaError_t launch_ksg_rows(const float4* X32, int natoms, int T, int i0, int Q, int Lpad, float* S, uint16_t* P,
-                            cudaStream_t s)
+cudaError_t launch_ksg_rows(const float4* X32, int natoms, int T, int i0, int Q, int Qp, int Lpad, float* S,
+                            uint16_t* P, cudaStream_t s)
 {
     int N2 = 256;
     while (N2 < T - 1)
@@ -938,26 +1008,72 @@ cudaError_t launch_ksg_rows(const float4* X32, int natoms, int T, int i0, int Q,
     const size_t smem = (size_t)N2 * 8 * (nbin ? 2 : 1) + (size_t)nbin * 8;
     // static shared memory comes on top of the dynamic part: always raise
     // the limit to what this launch needs
-    cudaFuncSetAttribute(ksg_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    ksg_rows_kernel<<<(unsigned)((long)natoms * Q), kRowsThreads, smem, s>>>(X32, T, i0, Q, Lpad, N2, nbin, S, P);
+    cudaError_t e = cudaFuncSetAttribute(ksg_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    ksg_rows_kernel<<<(unsigned)((long)natoms * Q), kRowsThreads, smem, s>>>(X32, T, i0, Q, Qp, Lpad, N2, nbin, S, P);
+    return cudaGetLastError();
+}
+
+// Shared memory budget of one CTA (the 227 KB opt-in maximum on sm_100, less
+// room for the static variables).
+constexpr size_t kSmemBudget = 226 * 1024;
+
+// Warps per CTA that fit the budget next to the staged coordinate rows, or 0.
+static int fit_warps(int T, size_t per_warp, int max_warps, int min_warps)
+{
+    const size_t rows = (size_t)2 * T * 16;
+    if (rows >= kSmemBudget)
+        return 0;
+    int w = (int)((kSmemBudget - rows) / per_warp);
+    w     = w > max_warps ? max_warps : w;
+    return w >= min_warps ? w : 0;
+}
+
+static cudaError_t launch_tasks(void (*kernel)(WalkParams), int max_warps, size_t per_warp, int sms, WalkParams p,
+                                cudaStream_t s)
+{
+    // stage the pair's coordinate rows in shared memory when enough warps fit
+    int warps = fit_warps(p.T, per_warp, max_warps, 8);
+    p.staged  = warps > 0 ? 1 : 0;
+    if (!p.staged)
+        warps = max_warps;
+    const size_t smem = (p.staged ? (size_t)2 * p.T * 16 : 0) + (size_t)warps * per_warp;
+    cudaError_t  e    = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    int per_sm = 0;
+    e          = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, warps * 32, smem);
+    if (e != cudaSuccess)
+        return e;
+    per_sm = per_sm < 1 ? 1 : per_sm;
+    kernel<<<sms * per_sm, warps * 32, smem, s>>>(p);
     return cudaGetLastError();
 }
 
 cudaError_t launch_ksg_walk(const WalkParams& p, int sms, cudaStream_t s)
 {
-    const size_t smem = (size_t)p.warp_smem * kWalkWarps;
-    cudaFuncSetAttribute(ksg_walk_kernel<kWalkWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return launch_tasks(ksg_walk_kernel, kWalkWarps, (size_t)kWalkBuckets * 32, sms, p, s);
+}
+
+cudaError_t launch_ksg_finish(const WalkParams& p, int sms, cudaStream_t s)
+{
+    const size_t smem = (size_t)kFinishWarps * kBandSlotBytes * kBandCap * 32;
+    cudaError_t  e    = cudaFuncSetAttribute(ksg_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ksg_walk_kernel<kWalkWarps>, kWalkWarps * 32, smem);
-    if (per_sm < 1)
-        per_sm = 1;
-    ksg_walk_kernel<kWalkWarps><<<sms * per_sm, kWalkWarps * 32, smem, s>>>(p);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ksg_finish_kernel, kFinishWarps * 32, smem);
+    if (e != cudaSuccess)
+        return e;
+    per_sm = per_sm < 1 ? 1 : per_sm;
+    ksg_finish_kernel<<<sms * per_sm, kFinishWarps * 32, smem, s>>>(p);
     return cudaGetLastError();
 }
 
-cudaError_t launch_ksg_queue(const QueueParams& p, int sms, cudaStream_t s)
+cudaError_t launch_ksg_fixup(const FixupParams& p, int sms, cudaStream_t s)
 {
-    ksg_queue_kernel<<<sms * 4, 256, 0, s>>>(p);
+    ksg_fixup_kernel<<<sms * 4, 256, 0, s>>>(p);
     return cudaGetLastError();
 }
 

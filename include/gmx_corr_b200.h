@@ -161,13 +161,14 @@ int gc_ksg_plan_is_fast(const gc_ksg_plan* plan);
 /* Queries of the last run that the fast path handed to the exact FP64
  * kernel (valid after gc_ksg_plan_sync). */
 long gc_ksg_plan_handoffs(const gc_ksg_plan* plan);
-/* Mean number of sorted-row entries the fast path walked per query in the
+/* Mean number of sorted-row entries the fast path walked per (pair, query) in the
  * last run (valid after gc_ksg_plan_sync; 0 for the exact path). */
 double gc_ksg_plan_walk_mean(const gc_ksg_plan* plan);
-/* Hand-overs of the last run by cause: 1 walk longer than the per-warp
- * buffer, 2 k-th value outside the histogram range, 3 band around the k-th
- * value too wide, 4 ambiguous set too large, 5 too many candidates for the
- * FP64 maxima (valid after gc_ksg_plan_sync). */
+/* Hand-overs of the last run by cause: 2 k-th value beyond the walk
+ * histogram's range, 3 band around the k-th value larger than the per-query
+ * store or inconsistent, 4 ambiguous set inconsistent or too large, 5 scan
+ * for the marginal maxima too long, 6 count band outside the walked prefix
+ * (valid after gc_ksg_plan_sync). */
 long gc_ksg_plan_handoff_reason(const gc_ksg_plan* plan, int reason);
 /* Device time in milliseconds of the neighbour-statistics kernel(s) of the
  * last run, measured with CUDA events on the run's stream (valid after the

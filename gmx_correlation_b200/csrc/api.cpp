@@ -53,7 +53,9 @@ struct gc_ksg_plan
     DevBuf<float4>               X32;
     DevBuf<float>                eps, S;
     DevBuf<uint16_t>             P;
-    DevBuf<unsigned long long>   task_counter, wres;
+    DevBuf<unsigned long long>   task_counter, wres, hq;
+    DevBuf<unsigned>             hq_len;
+    unsigned                     hq_cap = 0;
     DevBuf<int>                  pair_order; // task order of the local pairs (atom tiles)
     DevBuf<unsigned long long>   walk_elems;
     DevBuf<unsigned>             reasons;
@@ -181,6 +183,12 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
         GC_TRY(p->P.alloc((size_t)natoms * p->Qp * p->Lpad));
         GC_TRY(p->task_counter.alloc(2));
         GC_TRY(p->wres.alloc((size_t)p->Q * pc));
+        // hand-over queue: ample for the rare hand-overs; overflow is caught
+        // by the fix-up's scan of the counts
+        const double hq_want = 0.01 * (double)pc * T + 4096.0;
+        p->hq_cap            = (unsigned)(hq_want < 16777216.0 ? hq_want : 16777216.0);
+        GC_TRY(p->hq.alloc(p->hq_cap));
+        GC_TRY(p->hq_len.alloc(1));
         GC_TRY(p->walk_elems.alloc(1));
         GC_TRY(p->reasons.alloc(8));
     }
@@ -243,6 +251,7 @@ gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi
             GC_TRY_CUDA(gc::launch_ksg_x32(p->X.p, p->natoms, T, p->X32.p, p->eps.p, s));
             GC_TRY_CUDA(cudaMemsetAsync(p->reasons.p, 0, 8 * sizeof(unsigned), s));
             GC_TRY_CUDA(cudaMemsetAsync(p->walk_elems.p, 0, sizeof(unsigned long long), s));
+            GC_TRY_CUDA(cudaMemsetAsync(p->hq_len.p, 0, sizeof(unsigned), s));
             p->launches += 1;
             gc::WalkParams w{};
             w.X32          = p->X32.p;
@@ -261,6 +270,9 @@ gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi
             w.pair_order   = p->pair_order.p;
             w.shift        = p->shift;
             w.wres         = p->wres.p;
+            w.hq           = p->hq.p;
+            w.hq_len       = p->hq_len.p;
+            w.hq_cap       = p->hq_cap;
             w.cnt          = p->cnt.p;
             w.task_counter = p->task_counter.p;
             w.status       = p->status.p;
@@ -287,8 +299,11 @@ gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi
             fp.pair_count = p->pair_count;
             fp.pair_ab    = p->pair_ab.p;
             fp.cnt        = p->cnt.p;
+            fp.hq         = p->hq.p;
+            fp.hq_len     = p->hq_len.p;
+            fp.hq_cap     = p->hq_cap;
             GC_TRY_CUDA(gc::launch_ksg_fixup(fp, p->sms, s));
-            p->launches += 1;
+            p->launches += 2;
         }
         else
         {

@@ -145,11 +145,60 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(const float4* __
         kmin = min(kmin, red_min[w]);
         kmax = max(kmax, red_max[w]);
     }
-    // bucket = floor((key - kmin) * nbin / (kmax - kmin + 1)), in FP32: the
-    // conversion and the scaling are monotone, so buckets keep key order
-    const float scale = (float)nbin / ((float)(kmax - kmin) + 1.0f);
+    // Buckets follow the row's own distribution: a coarse 64-bin histogram
+    // (linear in the value) gives a piecewise-linear CDF, and a key's bucket
+    // is floor(CDF * nbin), so each bucket holds about one key and the
+    // per-bucket insertion sorts stay short and balanced.  Every step is
+    // monotone in the value (FP32 products and sums of non-negative terms,
+    // the fraction clamped to [0, 1]), so buckets keep key order.
+    __shared__ unsigned coarse[kRowsThreads / 32][64];
+    __shared__ float    cum[65];
+    const float vmin = __uint_as_float(kmin), vmax = __uint_as_float(kmax);
+    const float cinv = vmax > vmin ? 64.0f / (vmax - vmin) : 0.0f;
+    for (int e = lane; e < 64; e += 32)
+        coarse[warp][e] = 0u;
+    __syncwarp();
+    auto coarse_of = [&](float v, float& frac) -> unsigned {
+        const float    t = (v - vmin) * cinv;
+        const unsigned c = min((unsigned)t, 63u);
+        frac             = fminf(t - (float)c, 1.0f);
+        return c;
+    };
+    for (int m = tid; m < N && nbin; m += kRowsThreads)
+    {
+        float f;
+        atomicAdd(&coarse[warp][coarse_of(__uint_as_float((unsigned)(in[m] >> 32)), f)], 1u);
+    }
+    __syncthreads();
+    if (warp == 0)
+    {
+        // exclusive prefix over the 64 coarse bins (two per lane), as floats
+        unsigned c0 = 0u, c1 = 0u;
+        for (int w = 0; w < kRowsThreads / 32; ++w)
+        {
+            c0 += coarse[w][2 * lane];
+            c1 += coarse[w][2 * lane + 1];
+        }
+        unsigned incl = c0 + c1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const unsigned y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o)
+                incl += y;
+        }
+        const unsigned excl = incl - c0 - c1;
+        cum[2 * lane]       = (float)excl;
+        cum[2 * lane + 1]   = (float)(excl + c0);
+        if (lane == 31)
+            cum[64] = (float)incl;
+    }
+    __syncthreads();
+    const float fscale = (float)nbin / fmaxf((float)N, 1.0f);
     auto bin_of = [&](unsigned long long key) -> unsigned {
-        const unsigned b = (unsigned)((float)((unsigned)(key >> 32) - kmin) * scale);
+        float          f;
+        const unsigned c = coarse_of(__uint_as_float((unsigned)(key >> 32)), f);
+        const unsigned b = (unsigned)((cum[c] + f * (cum[c + 1] - cum[c])) * fscale);
         return b < (unsigned)nbin ? b : (unsigned)nbin - 1;
     };
     // histogram
@@ -407,31 +456,6 @@ __device__ __forceinline__ bool next_task(const WalkParams& p, unsigned long lon
     return true;
 }
 
-// Copies the coordinate rows of a1 and a2 into shared memory (sx[0, T) and
-// sx[T, 2T)) and returns their addresses; without staging, the global rows.
-__device__ __forceinline__ void pair_rows(const WalkParams& p, int a1, int a2, float4* sx, const float4*& xa,
-                                          const float4*& xb)
-{
-    if (p.staged)
-    {
-        const float4* ga = p.X32 + (size_t)a1 * p.T;
-        const float4* gb = p.X32 + (size_t)a2 * p.T;
-        for (int e = threadIdx.x; e < p.T; e += blockDim.x)
-        {
-            sx[e]       = ga[e];
-            sx[p.T + e] = gb[e];
-        }
-        __syncthreads();
-        xa = sx;
-        xb = sx + p.T;
-    }
-    else
-    {
-        xa = p.X32 + (size_t)a1 * p.T;
-        xb = p.X32 + (size_t)a2 * p.T;
-    }
-}
-
 // Walk result of one (pair, query): bucket of the k-th value, the number of
 // entries below that bucket, the walked length, and a hand-over cause.
 __device__ __forceinline__ unsigned long long pack_walk(int bstar, int prefix, int m_end, int reason)
@@ -442,88 +466,107 @@ __device__ __forceinline__ unsigned long long pack_walk(int bstar, int prefix, i
 
 } // namespace
 
-// Pass 1: walk the sorted row, histogram v = max(s, d) per lane.
+// Pass 1: walk the sorted row, histogram v = max(s, d) per lane.  STAGED:
+// the pair's coordinate rows are copied into shared memory per task.
+template <bool STAGED>
 __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkParams p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ long long s_task;
     const int            warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
     float4*              sx   = reinterpret_cast<float4*>(smem_raw);
-    unsigned char*       base = smem_raw + (p.staged ? (size_t)2 * p.T * 16 : 0) + (size_t)warp * kWalkBuckets * 32;
+    unsigned char*       base = smem_raw + (STAGED ? (size_t)2 * p.T * 16 : 0) + (size_t)warp * kWalkBuckets * 32;
     // bucket b of this lane: byte b % 4 of word (b / 4) * 32 + lane, so the
     // 32 lanes of a warp always hit 32 different banks
     uint8_t* hist = base + lane * 4;
     auto     H    = [hist](unsigned b) -> uint8_t& { return hist[(b >> 2) * 128 + (b & 3)]; };
 
-    const int       K = p.K, Llen = p.T - 1, shift = p.shift;
+    const int       T = p.T, K = p.K, Llen = T - 1, shift = p.shift;
     const int       ngroups = (p.Q + 31) >> 5;
     const long long total   = (long long)((ngroups + warps - 1) / warps) * p.pair_count;
     const float     inf     = __int_as_float(0x7f800000);
     Task            tk;
     while (next_task(p, p.task_counter, total, &s_task, tk))
     {
-        const float4* xa;
-        const float4* xb;
-        pair_rows(p, tk.a1, tk.a2, sx, xa, xb);
+        const float4* xa = p.X32 + (size_t)tk.a1 * T;
+        const float4* xb = p.X32 + (size_t)tk.a2 * T;
+        if (STAGED)
+        {
+            for (int e = threadIdx.x; e < T; e += blockDim.x)
+            {
+                sx[e]     = xa[e];
+                sx[T + e] = xb[e];
+            }
+            __syncthreads();
+            xa = sx;
+            xb = sx + T;
+        }
         const int       g    = tk.c * warps + warp;
         const int       iq   = g * 32 + lane;
         const bool      live = g < ngroups && iq < p.Q;
         const int       iql  = live ? iq : 0;
         const LaneSetup u    = lane_setup(p, tk.a1, tk.a2, iql, p.i0 + iql, xa, xb);
+        // the other atom's coordinate row (shared memory when staged)
+        const float4* X32o = STAGED ? (u.wx ? sx + T : sx) : u.X32o;
         {
             uint4* h4 = reinterpret_cast<uint4*>(base);
             for (int e = lane; e < kWalkBuckets * 32 / 16; e += 32)
                 h4[e] = make_uint4(0u, 0u, 0u, 0u);
         }
         __syncwarp();
-        bool saturated = false; // a 255-count bucket below the last one
 
         // Buckets are 2^shift float ulps above L; v < L counts in cnt_lo.  Every
         // 16 entries the buckets below the current value are final (later
         // entries have v >= s), so their running sum R decides the stop value.
-        int    m = 0, cnt_lo = 0, R = 0, thr = 0;
-        float  stop    = inf;
-        bool   walking = live;
-        float4 s4      = u.rw.s4(0);
-        uint2  j4      = u.rw.j4(0);
+        const float4* Sg = reinterpret_cast<const float4*>(u.rw.S); // 4-entry groups of this lane's row
+        const uint2*  Pg = reinterpret_cast<const uint2*>(u.rw.P);
+        const size_t  gs = (size_t)p.Qp;                            // group stride
+        int           m = 0, cnt_lo = 0, R = 0, thr = 0, grp = 0;
+        float         stop      = inf;
+        bool          saturated = false; // a bucket below the last one passed 255
+        bool          walking   = live;
+        float4        s4        = make_float4(inf, inf, inf, inf);
+        uint2         j4        = make_uint2(0u, 0u);
+        if (live)
+        {
+            s4 = Sg[0];
+            j4 = Pg[0];
+        }
+        const int last = (Llen - 1) >> 2; // the last (possibly partial) group
         while (walking)
         {
-            if (m >= Llen) // the whole row walked (m stays a multiple of 4 here)
+            if (grp > last) // the whole row walked
                 break;
-            float4 ns4 = s4;
-            uint2  nj4 = j4;
-            if (m + 4 < Llen) // prefetch the next group
-            {
-                ns4 = u.rw.s4((m >> 2) + 1);
-                nj4 = u.rw.j4((m >> 2) + 1);
-            }
-            const float    sv[4] = {s4.x, s4.y, s4.z, s4.w};
+            // prefetch the next group (the last group again at the end)
+            const int    nxt   = grp < last ? grp + 1 : grp;
+            const float4 ns4   = Sg[(size_t)nxt * gs];
+            const uint2  nj4   = Pg[(size_t)nxt * gs];
+            const int    valid = Llen - grp * 4; // entries of this group inside the row (>= 1)
+            const float  sv[4] = {s4.x, s4.y, s4.z, s4.w};
             const unsigned jv[4] = {j4.x & 0xFFFFu, j4.x >> 16, j4.y & 0xFFFFu, j4.y >> 16};
             int            ntk   = 0;
+            // Branch-free: every slot gathers (frame 0 when not taken) and
+            // updates its bucket by 0 or 1; taken entries form a prefix.
 #pragma unroll
             for (int q = 0; q < 4; ++q)
             {
-                if (m + q < Llen && sv[q] <= stop) // taken entries form a prefix
-                {
-                    ++ntk;
-                    const float v = fmaxf(sv[q], dist3f(u.xo, u.X32o[jv[q]]));
-                    if (v < u.L)
-                        ++cnt_lo;
-                    else
-                    {
-                        const unsigned b = min((__float_as_uint(v) - u.Lb) >> shift, (unsigned)kWalkBuckets - 1);
-                        const unsigned h = H(b);
-                        if (h < 255u)
-                            H(b) = (uint8_t)(h + 1u);
-                        else if (b < kWalkBuckets - 1)
-                            saturated = true;
-                    }
-                }
+                const bool     take  = q < valid && sv[q] <= stop;
+                const float    v     = fmaxf(sv[q], dist3f(u.xo, X32o[take ? jv[q] : 0u]));
+                const bool     below = v < u.L;
+                const bool     inc   = take && !below;
+                const unsigned b     = min((__float_as_uint(v) - u.Lb) >> shift, (unsigned)kWalkBuckets - 1);
+                uint8_t&       c     = H(b);
+                const unsigned h     = c;
+                c                    = (uint8_t)(h + (inc ? 1u : 0u));
+                saturated |= inc && h == 255u && b < kWalkBuckets - 1;
+                ntk += take;
+                cnt_lo += take && below;
             }
             m += ntk;
+            ++grp;
             if (ntk < 4)
                 walking = false;
-            else if (stop == inf && (m & 15) == 0)
+            else if (stop == inf && (grp & 3) == 0)
             {
                 const float sl = sv[3];
                 const int   bn =
@@ -950,6 +993,12 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkPa
                 atomicOr(p.status, kStatFallback);
                 if (p.reasons)
                     atomicAdd(p.reasons + reason, 1u);
+                if (p.hq)
+                {
+                    const unsigned q = atomicAdd(p.hq_len, 1u);
+                    if (q < p.hq_cap)
+                        p.hq[q] = (unsigned long long)i * p.pair_count + tk.pl;
+                }
             }
             p.cnt[(size_t)i * p.pair_count + tk.pl] = out;
         }
@@ -957,7 +1006,36 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkPa
     }
 }
 
-// Exact FP64 statistics for the queries the walk marked with kHandOver.
+// Exact FP64 statistics of one handed-over (query, pair): cnt index idx.
+__device__ __forceinline__ void fixup_one(const FixupParams& p, long long idx, unsigned* hist, int lane)
+{
+    const int  i  = (int)(idx / p.pair_count);
+    const long pl = (long)(idx - (long long)i * p.pair_count);
+    int        a1, a2;
+    if (p.pair_ab)
+    {
+        a1 = p.pair_ab[pl].x;
+        a2 = p.pair_ab[pl].y;
+    }
+    else
+        pair_from_index(p.pair_begin + pl, &a1, &a2);
+    const uint32_t c = exact_query(p.X64, p.T, p.K, a1, a2, i, p.box, p.rank_shift, hist, lane);
+    if (lane == 0)
+        p.cnt[idx] = c;
+    __syncwarp();
+}
+
+// The queued hand-overs, one warp each, spread over the whole grid.
+__global__ void __launch_bounds__(256) ksg_fixup_queue_kernel(FixupParams p)
+{
+    __shared__ unsigned hist[8][256];
+    const int      warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned n    = min(*p.hq_len, p.hq_cap);
+    for (unsigned e = blockIdx.x * 8 + warp; e < n; e += gridDim.x * 8)
+        fixup_one(p, (long long)p.hq[e], hist[warp], lane);
+}
+
+// Any kHandOver mark left (the queue overflowed, or no queue): scan cnt.
 __global__ void __launch_bounds__(256) ksg_fixup_kernel(FixupParams p)
 {
     __shared__ unsigned hist[8][256];
@@ -969,23 +1047,9 @@ __global__ void __launch_bounds__(256) ksg_fixup_kernel(FixupParams p)
         unsigned        hm = __ballot_sync(kFull, e < n && p.cnt[e] == kHandOver);
         while (hm)
         {
-            const int       src = __ffs(hm) - 1;
-            const long long idx = c0 + src;
+            const int src = __ffs(hm) - 1;
             hm &= hm - 1;
-            const int  i  = (int)(idx / p.pair_count);
-            const long pl = (long)(idx - (long long)i * p.pair_count);
-            int        a1, a2;
-            if (p.pair_ab)
-            {
-                a1 = p.pair_ab[pl].x;
-                a2 = p.pair_ab[pl].y;
-            }
-            else
-                pair_from_index(p.pair_begin + pl, &a1, &a2);
-            const uint32_t c = exact_query(p.X64, p.T, p.K, a1, a2, i, p.box, p.rank_shift, hist[warp], lane);
-            if (lane == 0)
-                p.cnt[idx] = c;
-            __syncwarp();
+            fixup_one(p, c0 + src, hist[warp], lane);
         }
     }
 }
@@ -1053,7 +1117,9 @@ static cudaError_t launch_tasks(void (*kernel)(WalkParams), int max_warps, size_
 
 cudaError_t launch_ksg_walk(const WalkParams& p, int sms, cudaStream_t s)
 {
-    return launch_tasks(ksg_walk_kernel, kWalkWarps, (size_t)kWalkBuckets * 32, sms, p, s);
+    const bool staged = fit_warps(p.T, (size_t)kWalkBuckets * 32, kWalkWarps, 8) > 0;
+    return launch_tasks(staged ? ksg_walk_kernel<true> : ksg_walk_kernel<false>, kWalkWarps,
+                        (size_t)kWalkBuckets * 32, sms, p, s);
 }
 
 cudaError_t launch_ksg_finish(const WalkParams& p, int sms, cudaStream_t s)
@@ -1073,6 +1139,13 @@ cudaError_t launch_ksg_finish(const WalkParams& p, int sms, cudaStream_t s)
 
 cudaError_t launch_ksg_fixup(const FixupParams& p, int sms, cudaStream_t s)
 {
+    if (p.hq)
+    {
+        ksg_fixup_queue_kernel<<<sms * 4, 256, 0, s>>>(p);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess)
+            return e;
+    }
     ksg_fixup_kernel<<<sms * 4, 256, 0, s>>>(p);
     return cudaGetLastError();
 }

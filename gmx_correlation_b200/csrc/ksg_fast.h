@@ -32,6 +32,9 @@ struct WalkParams
     int             shift;   // histogram bucket = 2^shift float ulps above the lower bound
     uint32_t*       cnt;     // [T][pair_count] n_x | n_y << 16, or kHandOver
     unsigned long long* wres;         // [Q][pair_count] walk results of the block
+    unsigned long long* hq;           // hand-over queue: cnt indices i * pair_count + pl
+    unsigned*           hq_len;
+    unsigned            hq_cap;
     unsigned long long* task_counter; // [2]: walk, finish
     int*                status;
     unsigned long long* walk_elems; // optional: total walked row entries
@@ -45,6 +48,9 @@ struct FixupParams
     long          pair_begin, pair_count;
     const int2*   pair_ab;
     uint32_t*     cnt;
+    const unsigned long long* hq; // hand-over queue (may be null): entries are cnt indices
+    const unsigned*           hq_len;
+    unsigned                  hq_cap;
 };
 
 // Bucket width of the walk histogram for k: about 1.3/k of the value
@@ -63,6 +69,8 @@ cudaError_t launch_ksg_rows(const float4* X32, int natoms, int T, int i0, int Q,
                             uint16_t* P, cudaStream_t s);
 cudaError_t launch_ksg_walk(const WalkParams& p, int sms, cudaStream_t s);
 cudaError_t launch_ksg_finish(const WalkParams& p, int sms, cudaStream_t s);
+// Exact FP64 statistics for every queued hand-over, then for any hand-over
+// mark the queue could not hold (a scan of cnt).
 cudaError_t launch_ksg_fixup(const FixupParams& p, int sms, cudaStream_t s);
 
 } // namespace gc

@@ -30,7 +30,7 @@ __all__ = [
     "gcmi_corrmatrix", "te_matrix", "kraskov_prepare", "kraskov_wrap", "pearsify",
     "write_matrix", "write_xpm_matrix", "read_matrix", "KsgPlan", "PATH_AUTO",
     "PATH_EXACT_FP64", "LIB_PATH", "probe_fp32", "screen_features", "ScreenModel", "ksg_screened",
-    "SCREEN_IN", "SCREEN_RAW", "SCREEN_BASE", "SCREEN_COMP",
+    "SCREEN_IN", "SCREEN_RAW", "SCREEN_BASE", "SCREEN_COMP", "release_cache",
 ]
 
 LIB_PATH = Path(__file__).resolve().parent / "libgmxcorr_b200.so"
@@ -131,6 +131,7 @@ def lib() -> ctypes.CDLL:
                                              ctypes.c_void_p, ctypes.c_void_p]
         L.gc_ksg_plan_destroy.argtypes = [ctypes.c_void_p]
         L.gc_ksg_plan_destroy.restype = None
+        L.gc_release_cache.restype = None
         fp = ctypes.POINTER(ctypes.c_float)
         L.gc_screen_features.argtypes = [ctypes.POINTER(_TrajView), ctypes.c_int, ctypes.POINTER(_Opts), fp, fp, fp]
         L.gc_screen_model_create.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
@@ -233,6 +234,11 @@ def kraskov_corrmatrix(x, k: int, *, path: int = PATH_AUTO, device: int = -1, pa
     _check(lib().gc_ksg_matrix(ctypes.byref(v), int(k), ctypes.byref(o), _dptr(out)))
     mat = out.reshape(n, n)
     return (mat, nx, ny) if detail else mat
+
+
+def release_cache() -> None:
+    """Free the device workspace kraskov_corrmatrix keeps between calls."""
+    lib().gc_release_cache()
 
 
 def gauss_corrmatrix(x, *, device: int = -1) -> np.ndarray:

@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -57,6 +58,7 @@ struct gc_ksg_plan
     DevBuf<unsigned>             hq_len;
     unsigned                     hq_cap = 0;
     DevBuf<int>                  pair_order; // task order of the local pairs (atom tiles)
+    DevBuf<double>               io_xyz, io_mi; // gc_ksg_matrix staging of inputs and outputs
     DevBuf<unsigned long long>   walk_elems;
     DevBuf<unsigned>             reasons;
     long                         reason_counts[8] = {};
@@ -398,8 +400,84 @@ void gc_ksg_plan_destroy(gc_ksg_plan* p)
         p->task_counter.reset();
         p->walk_elems.reset();
         p->reasons.reset();
+        delete p; // the remaining buffers are freed with this device current
     }
-    delete p;
+}
+
+} // extern "C"
+
+namespace {
+
+// One cached plan per device for gc_ksg_matrix: a repeated call with the same
+// shape (atoms, frames, k, path, pair range) reuses the plan's device
+// workspace instead of allocating and freeing it again.  Explicit pair lists
+// are not cached.  gc_release_cache() frees the cached plans.
+struct PlanKey
+{
+    int  natoms = 0, nframes = 0, k = 0, path = 0;
+    long pair_begin = 0, pair_count = 0;
+    bool operator==(const PlanKey& o) const
+    {
+        return natoms == o.natoms && nframes == o.nframes && k == o.k && path == o.path &&
+               pair_begin == o.pair_begin && pair_count == o.pair_count;
+    }
+};
+
+constexpr int kCacheDevices = 64;
+std::mutex    g_cache_mutex;
+gc_ksg_plan*  g_cache_plan[kCacheDevices] = {};
+PlanKey       g_cache_key[kCacheDevices];
+
+// Takes the cached plan for (device, key) if there is one, else nullptr.
+gc_ksg_plan* cache_take(int dev, const PlanKey& key)
+{
+    if (dev < 0 || dev >= kCacheDevices)
+        return nullptr;
+    std::lock_guard<std::mutex> lock(g_cache_mutex);
+    if (g_cache_plan[dev] && g_cache_key[dev] == key)
+    {
+        gc_ksg_plan* p    = g_cache_plan[dev];
+        g_cache_plan[dev] = nullptr;
+        return p;
+    }
+    return nullptr;
+}
+
+// Returns a plan to the cache; an older cached plan of that device is freed.
+void cache_put(int dev, const PlanKey& key, gc_ksg_plan* p)
+{
+    gc_ksg_plan* old = nullptr;
+    if (dev >= 0 && dev < kCacheDevices)
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mutex);
+        old               = g_cache_plan[dev];
+        g_cache_plan[dev] = p;
+        g_cache_key[dev]  = key;
+    }
+    else
+        old = p;
+    if (old)
+        gc_ksg_plan_destroy(old);
+}
+
+} // namespace
+
+extern "C" {
+
+void gc_release_cache(void)
+{
+    gc_ksg_plan* plans[kCacheDevices];
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mutex);
+        for (int d = 0; d < kCacheDevices; ++d)
+        {
+            plans[d]        = g_cache_plan[d];
+            g_cache_plan[d] = nullptr;
+        }
+    }
+    for (gc_ksg_plan* p : plans)
+        if (p)
+            gc_ksg_plan_destroy(p);
 }
 
 gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, double* mi)
@@ -413,19 +491,32 @@ gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, do
     GC_TRY(validate_ksg(n, T, k, o, &pb, &pc));
     DeviceScope dev(o.device);
     GC_TRY(dev.st);
-    gc_ksg_plan* raw = nullptr;
-    GC_TRY(gc_ksg_plan_create(n, T, k, &o, &raw));
+    int cur = -1;
+    cudaGetDevice(&cur);
+    PlanKey key;
+    key.natoms     = n;
+    key.nframes    = T;
+    key.k          = k;
+    key.path       = o.path;
+    key.pair_begin = pb;
+    key.pair_count = pc;
+    const bool   cacheable = o.pair_list == nullptr;
+    gc_ksg_plan* raw       = cacheable ? cache_take(cur, key) : nullptr;
+    if (!raw)
+        GC_TRY(gc_ksg_plan_create(n, T, k, &o, &raw));
     std::unique_ptr<gc_ksg_plan, void (*)(gc_ksg_plan*)> plan(raw, gc_ksg_plan_destroy);
-    DevBuf<double> d_xyz, d_mi;
-    GC_TRY(d_xyz.alloc((size_t)n * T * 3));
-    GC_TRY(d_mi.alloc((size_t)(pc > 0 ? pc : 1)));
+    if (!plan->io_xyz.p)
+    {
+        GC_TRY(plan->io_xyz.alloc((size_t)n * T * 3));
+        GC_TRY(plan->io_mi.alloc((size_t)(pc > 0 ? pc : 1)));
+    }
     cudaStream_t s = plan->stream;
-    GC_TRY(upload_traj(traj, d_xyz.p, s));
-    GC_TRY(gc_ksg_plan_run(plan.get(), d_xyz.p, d_mi.p, s));
+    GC_TRY(upload_traj(traj, plan->io_xyz.p, s));
+    GC_TRY(gc_ksg_plan_run(plan.get(), plan->io_xyz.p, plan->io_mi.p, s));
     GC_TRY(gc_ksg_plan_sync(plan.get()));
     std::vector<double> pm((size_t)pc);
     if (pc > 0)
-        GC_TRY_CUDA(cudaMemcpy(pm.data(), d_mi.p, sizeof(double) * pc, cudaMemcpyDeviceToHost));
+        GC_TRY_CUDA(cudaMemcpy(pm.data(), plan->io_mi.p, sizeof(double) * pc, cudaMemcpyDeviceToHost));
     if (o.detail_nx || o.detail_ny)
     {
         std::vector<uint32_t> c((size_t)T * pc);
@@ -452,6 +543,8 @@ gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, do
         mi[(size_t)a1 * n + a2] = pm[(size_t)pl];
         mi[(size_t)a2 * n + a1] = pm[(size_t)pl];
     }
+    if (cacheable)
+        cache_put(cur, key, plan.release());
     return GC_OK;
 }
 

@@ -86,11 +86,13 @@ __global__ void ksg_x32_kernel(const double* __restrict__ X64, int natoms, int T
 
 // One CTA per (atom, query): the row's T-1 marginal distances (self
 // excluded), sorted ascending with their frames.  Keys are
-// (distance bits << 32 | frame); a bucket pass over the row's key range
-// (histogram, scan, scatter) leaves a few keys per bucket, which one thread
-// per bucket insertion-sorts.  A row with a crowded bucket (more than 64
-// equal-ish distances, e.g. duplicated frames) is sorted by a bitonic
-// network over the same buffer instead.
+// (distance bits << 32 | frame).  A bucket pass over the row's own
+// distribution (range, coarse CDF, histogram, scan, scatter) leaves about one
+// key per bucket, which one thread per bucket insertion-sorts.  Distances are
+// recomputed from the atom's coordinate row (L1-resident) in every pass
+// rather than kept in shared memory.  A row with a crowded bucket (more than
+// 64 equal-ish distances, e.g. duplicated frames), and rows longer than 8192,
+// are sorted by a bitonic network instead.
 constexpr int kRowsThreads = 256;
 
 __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(const float4* __restrict__ X32, int T, int i0, int Q,
@@ -98,32 +100,35 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(const float4* __
                                                                 float* __restrict__ S, uint16_t* __restrict__ P)
 {
     extern __shared__ __align__(16) unsigned char rows_smem[];
-    unsigned long long* keys   = reinterpret_cast<unsigned long long*>(rows_smem);      // [N2] sorted output
-    unsigned long long* in     = keys + N2;                                             // [N2] unsorted (bucket path)
-    unsigned*           hist   = reinterpret_cast<unsigned*>(in + (nbin ? N2 : 0));     // [nbin]
-    unsigned*           cursor = hist + nbin;                                           // [nbin]
+    unsigned long long* keys   = reinterpret_cast<unsigned long long*>(rows_smem); // [N2] sorted output
+    unsigned*           hist   = reinterpret_cast<unsigned*>(keys + N2);           // [nbin]
+    unsigned*           cursor = hist + nbin;                                      // [nbin]
     __shared__ unsigned red_min[kRowsThreads / 32], red_max[kRowsThreads / 32];
+    __shared__ unsigned coarse[kRowsThreads / 32][64];
+    __shared__ float    cum[65];
     __shared__ int      crowded;
 
-    const int    row = blockIdx.x;
-    const int    a   = row / Q;
-    const int    iq  = row - a * Q;
-    const int    i   = i0 + iq;
-    const int    N   = T - 1;
-    const int    tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const float4 q   = X32[(size_t)a * T + i];
+    const int     row = blockIdx.x;
+    const int     a   = row / Q;
+    const int     iq  = row - a * Q;
+    const int     i   = i0 + iq;
+    const int     N   = T - 1;
+    const int     tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const float4* xr  = X32 + (size_t)a * T;
+    const float4  q   = xr[i];
+    auto          frame_of = [i](int m) { return m < i ? m : m + 1; };
 
     unsigned kmin = 0xFFFFFFFFu, kmax = 0u;
     for (int m = tid; m < N; m += kRowsThreads)
     {
-        const int      j = m < i ? m : m + 1;
-        const unsigned k = __float_as_uint(dist3f(q, X32[(size_t)a * T + j]));
-        (nbin ? in : keys)[m] = ((unsigned long long)k << 32) | (unsigned)j;
+        const unsigned k = __float_as_uint(dist3f(q, xr[frame_of(m)]));
         kmin             = min(kmin, k);
         kmax             = max(kmax, k);
     }
     for (int b = tid; b < nbin; b += kRowsThreads)
         hist[b] = 0u;
+    for (int e = lane; e < 64; e += 32)
+        coarse[warp][e] = 0u;
     if (tid == 0)
         crowded = nbin == 0; // no bucket pass for very long rows
 #pragma unroll
@@ -151,13 +156,8 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(const float4* __
     // per-bucket insertion sorts stay short and balanced.  Every step is
     // monotone in the value (FP32 products and sums of non-negative terms,
     // the fraction clamped to [0, 1]), so buckets keep key order.
-    __shared__ unsigned coarse[kRowsThreads / 32][64];
-    __shared__ float    cum[65];
     const float vmin = __uint_as_float(kmin), vmax = __uint_as_float(kmax);
     const float cinv = vmax > vmin ? 64.0f / (vmax - vmin) : 0.0f;
-    for (int e = lane; e < 64; e += 32)
-        coarse[warp][e] = 0u;
-    __syncwarp();
     auto coarse_of = [&](float v, float& frac) -> unsigned {
         const float    t = (v - vmin) * cinv;
         const unsigned c = min((unsigned)t, 63u);
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(const float4* __
     for (int m = tid; m < N && nbin; m += kRowsThreads)
     {
         float f;
-        atomicAdd(&coarse[warp][coarse_of(__uint_as_float((unsigned)(in[m] >> 32)), f)], 1u);
+        atomicAdd(&coarse[warp][coarse_of(dist3f(q, xr[frame_of(m)]), f)], 1u);
     }
     __syncthreads();
     if (warp == 0)
@@ -195,15 +195,15 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(const float4* __
     }
     __syncthreads();
     const float fscale = (float)nbin / fmaxf((float)N, 1.0f);
-    auto bin_of = [&](unsigned long long key) -> unsigned {
+    auto bin_of = [&](float v) -> unsigned {
         float          f;
-        const unsigned c = coarse_of(__uint_as_float((unsigned)(key >> 32)), f);
+        const unsigned c = coarse_of(v, f);
         const unsigned b = (unsigned)((cum[c] + f * (cum[c + 1] - cum[c])) * fscale);
         return b < (unsigned)nbin ? b : (unsigned)nbin - 1;
     };
     // histogram
     for (int m = tid; m < N && nbin; m += kRowsThreads)
-        atomicAdd(&hist[bin_of(in[m])], 1u);
+        atomicAdd(&hist[bin_of(dist3f(q, xr[frame_of(m)]))], 1u);
     __syncthreads();
     // exclusive scan of hist into cursor (each thread a contiguous slice)
     const int per = nbin / kRowsThreads; // 0 without a bucket pass
@@ -227,26 +227,25 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(const float4* __
     unsigned run = wbase + incl - loc;
     for (int e = 0; e < per; ++e)
     {
-        const unsigned c       = hist[tid * per + e];
-        cursor[tid * per + e]  = run;
+        const unsigned c      = hist[tid * per + e];
+        cursor[tid * per + e] = run;
         if (c > 64)
             crowded = 1;
         run += c;
     }
     __syncthreads();
-    // scatter
-    if (!crowded)
-        for (int m = tid; m < N; m += kRowsThreads)
-        {
-            const unsigned long long k   = in[m];
-            const unsigned           pos = atomicAdd(&cursor[bin_of(k)], 1u);
-            keys[pos]                    = k;
-        }
-    else if (nbin)
-        for (int m = tid; m < N; m += kRowsThreads)
-            keys[m] = in[m];
+    // scatter (or place in frame order for the bitonic network)
+    const bool bucketed = !crowded;
+    for (int m = tid; m < N; m += kRowsThreads)
+    {
+        const int                j   = frame_of(m);
+        const float              d   = dist3f(q, xr[j]);
+        const unsigned long long k   = ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)j;
+        const unsigned           pos = bucketed ? atomicAdd(&cursor[bin_of(d)], 1u) : (unsigned)m;
+        keys[pos]                    = k;
+    }
     __syncthreads();
-    if (!crowded)
+    if (bucketed)
     {
         // cursor[b] now holds the end of bucket b; sort each bucket
         for (int e = 0; e < per; ++e)
@@ -277,8 +276,8 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(const float4* __
             {
                 for (int t = tid; t < (N2 >> 1); t += kRowsThreads)
                 {
-                    const int idx = ((t / j) * (j << 1)) + (t % j);
-                    const int prt = idx + j;
+                    const int                idx = ((t / j) * (j << 1)) + (t % j);
+                    const int                prt = idx + j;
                     const unsigned long long x = keys[idx], y = keys[prt];
                     if ((x > y) == ((idx & k) == 0))
                     {
@@ -302,7 +301,6 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(const float4* __
     }
 }
 
-
 namespace {
 
 // One lane's view of a transposed sorted row (see WalkParams).
@@ -320,6 +318,17 @@ struct LaneRow
     }
     __device__ __forceinline__ uint2 j4(int g) const { return *reinterpret_cast<const uint2*>(P + (size_t)g * gstride); }
 };
+
+// Entry q (0..3) of a 4-entry group: its distance and its frame.
+__device__ __forceinline__ float f4get(const float4& v, int q)
+{
+    return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+}
+
+__device__ __forceinline__ unsigned u2get16(const uint2& v, int q)
+{
+    return q < 2 ? ((v.x >> (16 * q)) & 0xFFFFu) : ((v.y >> (16 * (q - 2))) & 0xFFFFu);
+}
 
 __device__ __forceinline__ LaneRow lane_row(const WalkParams& p, int atom, int iq)
 {
@@ -710,47 +719,58 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkPa
                     ++nband;
                     nlo += v < elo;
                 };
-                // Both ranges in batches of 8: the row loads of a batch, then
-                // its gathers, then the tests, so the loads overlap.
-                for (int m0 = mw0; m0 < mw1; m0 += 8) // s in the band, d <= bandhi
+                // Both ranges by aligned 4-entry groups of the row (one 16-byte
+                // and one 8-byte load per group), two groups per round, so the
+                // loads of a round and then its gathers overlap.
+                for (int g0 = mw0 >> 2; g0 * 4 < mw1; g0 += 2) // s in the band, d <= bandhi
                 {
-                    int   jj[8];
-                    float sv[8], dv[8];
+                    float4 s4[2];
+                    uint2  j4[2];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        if (m0 + q < mw1)
+                    for (int h = 0; h < 2; ++h)
+                        if ((g0 + h) * 4 < mw1)
                         {
-                            jj[q] = rw.j(m0 + q);
-                            sv[q] = rw.s(m0 + q);
+                            s4[h] = rw.s4(g0 + h);
+                            j4[h] = rw.j4(g0 + h);
                         }
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        if (m0 + q < mw1)
-                            dv[q] = dist3f(xo, X32o[jj[q]]);
+                    for (int h = 0; h < 2; ++h)
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        if (m0 + q < mw1 && dv[q] <= bandhi)
-                            add(fmaxf(sv[q], dv[q]), sv[q], dv[q], jj[q], m0 + q);
+                        for (int q = 0; q < 4; ++q)
+                        {
+                            const int   mm = (g0 + h) * 4 + q;
+                            const bool  in = mm >= mw0 && mm < mw1;
+                            const int   j  = (int)u2get16(j4[h], q);
+                            const float sv = f4get(s4[h], q);
+                            const float dv = dist3f(xo, X32o[in ? j : 0]);
+                            if (in && dv <= bandhi)
+                                add(fmaxf(sv, dv), sv, dv, j, mm);
+                        }
                 }
-                for (int m0 = mo0; m0 < mo1; m0 += 8) // d in the band, s < inlo
+                for (int g0 = mo0 >> 2; g0 * 4 < mo1; g0 += 2) // d in the band, s < inlo
                 {
-                    int   jj[8];
-                    float sv[8], dv[8];
+                    float4 d4[2];
+                    uint2  j4[2];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        if (m0 + q < mo1)
+                    for (int h = 0; h < 2; ++h)
+                        if ((g0 + h) * 4 < mo1)
                         {
-                            jj[q] = ro.j(m0 + q);
-                            dv[q] = ro.s(m0 + q);
+                            d4[h] = ro.s4(g0 + h);
+                            j4[h] = ro.j4(g0 + h);
                         }
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        if (m0 + q < mo1)
-                            sv[q] = dist3f(xw, X32w[jj[q]]);
+                    for (int h = 0; h < 2; ++h)
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        if (m0 + q < mo1 && sv[q] < inlo)
-                            add(dv[q], sv[q], dv[q], jj[q], -1 - (m0 + q));
+                        for (int q = 0; q < 4; ++q)
+                        {
+                            const int   mm = (g0 + h) * 4 + q;
+                            const bool  in = mm >= mo0 && mm < mo1;
+                            const int   j  = (int)u2get16(j4[h], q);
+                            const float dv = f4get(d4[h], q);
+                            const float sv = dist3f(xw, X32w[in ? j : 0]);
+                            if (in && sv < inlo)
+                                add(dv, sv, dv, j, -1 - mm);
+                        }
                 }
                 int       n_in = prefix - nlo; // #{v < inlo}
                 const int r    = K - n_in;     // 1-based rank of the k-th value in the band
@@ -869,38 +889,35 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkPa
                             sec = val;
                     }
                     // members with v < inlo: the first one below the band start
-                    // in this row holds their maximum (four entries per round)
+                    // in this row holds their maximum (a 4-entry group per round)
                     int   mm = (side == 0 ? mw0 : mo0) - 1, first = -1;
                     float fval = -1.0f, fsec = -1.0f;
                     while (mm >= 0 && first < 0)
                     {
-                        int   jj[4];
-                        float sv[4];
+                        const int    g  = mm >> 2;
+                        const float4 s4 = row.s4(g);
+                        const uint2  j4 = row.j4(g);
+                        bool         ok[4];
 #pragma unroll
                         for (int q = 0; q < 4; ++q)
-                            if (mm - q >= 0)
-                            {
-                                jj[q] = row.j(mm - q);
-                                sv[q] = row.s(mm - q);
-                            }
-                        bool ok[4];
+                        {
+                            const bool in = g * 4 + q <= mm;
+                            ok[q] = in && dist3f(xc, Xc[in ? u2get16(j4, q) : 0u]) < inlo;
+                        }
 #pragma unroll
-                        for (int q = 0; q < 4; ++q)
-                            ok[q] = mm - q >= 0 && dist3f(xc, Xc[jj[q]]) < inlo;
-#pragma unroll
-                        for (int q = 0; q < 4; ++q)
+                        for (int q = 3; q >= 0; --q)
                             if (ok[q])
                             {
                                 if (first < 0)
                                 {
-                                    first = mm - q;
-                                    fval  = sv[q];
+                                    first = g * 4 + q;
+                                    fval  = f4get(s4, q);
                                 }
                                 else
-                                    fsec = fmaxf(fsec, sv[q]);
+                                    fsec = fmaxf(fsec, f4get(s4, q));
                             }
-                        mm -= 4; // the next unexamined position
-                        steps += 4;
+                        steps += mm - g * 4 + 1;
+                        mm = g * 4 - 1; // the next unexamined position
                         if (first < 0 && steps > kScanCap)
                             reason = kReasonScan;
                     }
@@ -1066,10 +1083,10 @@ cudaError_t launch_ksg_rows(const float4* X32, int natoms, int T, int i0, int Q,
     int N2 = 256;
     while (N2 < T - 1)
         N2 <<= 1;
-    // bucket pass up to 8192 keys (two key arrays + bins); longer rows use
-    // the bitonic network alone
+    // bucket pass up to 8192 keys (keys + bins); longer rows use the bitonic
+    // network alone
     const int    nbin = N2 <= 8192 ? (N2 < 4096 ? N2 : 4096) : 0;
-    const size_t smem = (size_t)N2 * 8 * (nbin ? 2 : 1) + (size_t)nbin * 8;
+    const size_t smem = (size_t)N2 * 8 + (size_t)nbin * 8;
     // static shared memory comes on top of the dynamic part: always raise
     // the limit to what this launch needs
     cudaError_t e = cudaFuncSetAttribute(ksg_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

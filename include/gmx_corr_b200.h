@@ -100,6 +100,12 @@ int gc_gpu_available(void);
  * the diagonal are written; the rest stays zero.  mi: natoms*natoms. */
 gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, double* mi);
 
+/* gc_ksg_matrix keeps the device workspace of its last call on each device
+ * (a few GB at 247 atoms x 2000 frames) and reuses it when the next call has
+ * the same shape (atoms, frames, k, path, pair range); explicit pair lists are
+ * not kept.  gc_release_cache frees every kept workspace. */
+void gc_release_cache(void);
+
 /* Gaussian (linearized) MI matrix.  Replaces gauss_corrmatrix
  * (lib/correlation_core.h:76, lib/correlation_core.cpp:280-311). */
 gc_status gc_gauss_matrix(const gc_traj_view* traj, const gc_opts* opts, double* mi);

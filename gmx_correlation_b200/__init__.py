@@ -30,7 +30,8 @@ __all__ = [
     "gcmi_corrmatrix", "te_matrix", "kraskov_prepare", "kraskov_wrap", "pearsify",
     "write_matrix", "write_xpm_matrix", "read_matrix", "KsgPlan", "PATH_AUTO",
     "PATH_EXACT_FP64", "LIB_PATH", "probe_fp32", "screen_features", "ScreenModel", "ksg_screened",
-    "SCREEN_IN", "SCREEN_RAW", "SCREEN_BASE", "SCREEN_COMP", "release_cache",
+    "SCREEN_IN", "SCREEN_RAW", "SCREEN_BASE", "SCREEN_COMP", "release_cache", "ksg_batch",
+    "ksg_batch_release",
 ]
 
 LIB_PATH = Path(__file__).resolve().parent / "libgmxcorr_b200.so"
@@ -132,6 +133,9 @@ def lib() -> ctypes.CDLL:
         L.gc_ksg_plan_destroy.argtypes = [ctypes.c_void_p]
         L.gc_ksg_plan_destroy.restype = None
         L.gc_release_cache.restype = None
+        L.gc_ksg_batch.argtypes = [ctypes.POINTER(_TrajView), ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                   ctypes.POINTER(_Opts), ctypes.POINTER(dp)]
+        L.gc_ksg_batch_release.restype = None
         fp = ctypes.POINTER(ctypes.c_float)
         L.gc_screen_features.argtypes = [ctypes.POINTER(_TrajView), ctypes.c_int, ctypes.POINTER(_Opts), fp, fp, fp]
         L.gc_screen_model_create.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
@@ -234,6 +238,35 @@ def kraskov_corrmatrix(x, k: int, *, path: int = PATH_AUTO, device: int = -1, pa
     _check(lib().gc_ksg_matrix(ctypes.byref(v), int(k), ctypes.byref(o), _dptr(out)))
     mat = out.reshape(n, n)
     return (mat, nx, ny) if detail else mat
+
+
+def ksg_batch(trajs, ks, *, device: int = -1):
+    """KSG MI matrices of several trajectories in one batched GPU run.
+
+    ``trajs``: list of (natoms_i, nframes_i, 3) mean-centred arrays; ``ks``:
+    one k per trajectory (or a single int).  Returns the list of matrices.
+    """
+    xs = [_coords(x) for x in trajs]
+    if isinstance(ks, int):
+        ks = [ks] * len(xs)
+    if len(ks) != len(xs):
+        raise ValueError("one k per trajectory")
+    views = (_TrajView * len(xs))()
+    for v, x in zip(views, xs):
+        v.natoms, v.nframes = x.shape[0], x.shape[1]
+        v.xyz = _dptr(x)
+        v.rows = None
+    outs = [np.zeros((x.shape[0], x.shape[0])) for x in xs]
+    ptrs = (ctypes.POINTER(ctypes.c_double) * len(xs))(*[_dptr(m) for m in outs])
+    karr = (ctypes.c_int * len(xs))(*[int(k) for k in ks])
+    o = _opts(device)
+    _check(lib().gc_ksg_batch(views, karr, len(xs), ctypes.byref(o), ptrs))
+    return outs
+
+
+def ksg_batch_release() -> None:
+    """Free the device workspace and graph the last ksg_batch kept."""
+    lib().gc_ksg_batch_release()
 
 
 def release_cache() -> None:

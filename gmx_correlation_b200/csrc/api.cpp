@@ -10,6 +10,7 @@
 #include "gc_geom.h"
 #include "ksg_fast.h"
 #include "host_common.h"
+#include "ksg_host.h"
 
 #include <cuda_runtime.h>
 
@@ -49,18 +50,10 @@ struct gc_ksg_plan
     int              launches = 0;
     cudaEvent_t      ev0 = nullptr, ev1 = nullptr;
     // fast path workspace
-    bool                         fast = false;
-    int                          Q = 0, Qp = 0, Lpad = 0, shift = 0;
-    DevBuf<float4>               X32;
-    DevBuf<float>                eps, S;
-    DevBuf<uint16_t>             P;
-    DevBuf<unsigned long long>   task_counter, wres, hq;
-    DevBuf<unsigned>             hq_len;
-    unsigned                     hq_cap = 0;
-    DevBuf<int>                  pair_order; // task order of the local pairs (atom tiles)
-    DevBuf<double>               io_xyz, io_mi; // gc_ksg_matrix staging of inputs and outputs
-    DevBuf<unsigned long long>   walk_elems;
-    DevBuf<unsigned>             reasons;
+    bool                  fast = false;
+    gc::host::KsgTraj     ft;
+    gc::host::KsgLaunch   fl;
+    DevBuf<double>        io_xyz, io_mi; // gc_ksg_matrix staging of inputs and outputs
     long                         reason_counts[8] = {};
     double                       walk_mean = 0.0;
     long                         handoffs = 0;
@@ -168,32 +161,6 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
     // The fast path sorts each marginal row in shared memory (<= 16384
     // frames); longer trajectories use the exact kernels throughout.
     p->fast = o.path != GC_PATH_EXACT_FP64 && nframes - 1 <= 16384 && pc > 0;
-    if (p->fast)
-    {
-        const int    T      = nframes;
-        p->Lpad             = ((T - 1) + 31) & ~31;
-        const double row    = (double)natoms * p->Lpad * 6.0;
-        const double budget = 8.0 * (1 << 30); // sorted rows of one query block
-        long         q      = (long)(budget / row) / 32 * 32;
-        q                   = q < 32 ? 32 : q;
-        p->Q                = (int)(q > T ? T : q);
-        p->Qp               = (p->Q + 31) & ~31;
-        p->shift            = gc::walk_histogram_shift(k);
-        GC_TRY(p->X32.alloc((size_t)natoms * T));
-        GC_TRY(p->eps.alloc((size_t)natoms));
-        GC_TRY(p->S.alloc((size_t)natoms * p->Qp * p->Lpad));
-        GC_TRY(p->P.alloc((size_t)natoms * p->Qp * p->Lpad));
-        GC_TRY(p->task_counter.alloc(2));
-        GC_TRY(p->wres.alloc((size_t)p->Q * pc));
-        // hand-over queue: ample for the rare hand-overs; overflow is caught
-        // by the fix-up's scan of the counts
-        const double hq_want = 0.01 * (double)pc * T + 4096.0;
-        p->hq_cap            = (unsigned)(hq_want < 16777216.0 ? hq_want : 16777216.0);
-        GC_TRY(p->hq.alloc(p->hq_cap));
-        GC_TRY(p->hq_len.alloc(1));
-        GC_TRY(p->walk_elems.alloc(1));
-        GC_TRY(p->reasons.alloc(8));
-    }
     const std::vector<double> psi = digamma_table(nframes);
     GC_TRY_CUDA(cudaMemcpy(p->psi.p, psi.data(), sizeof(double) * psi.size(), cudaMemcpyHostToDevice));
     if (o.pair_list && pc > 0)
@@ -208,23 +175,15 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
         GC_TRY(p->pair_ab.alloc((size_t)pc));
         GC_TRY_CUDA(cudaMemcpy(p->pair_ab.p, ab.data(), sizeof(int2) * ab.size(), cudaMemcpyHostToDevice));
     }
-    if (p->fast && pc > 0)
+    if (p->fast)
     {
-        // Walk tasks visit the pairs tile by tile (16 x 16 atoms), so the
-        // sorted rows of the atoms the running tasks read stay in L2.
-        std::vector<long long> key((size_t)pc);
-        for (long q = 0; q < pc; ++q)
-        {
-            int a1, a2;
-            gc::pair_from_index(o.pair_list ? (long)o.pair_list[q] : pb + q, &a1, &a2);
-            key[(size_t)q] = (((long long)(a1 >> 4) * 65536 + (a2 >> 4)) << 32) | (long long)q;
-        }
-        std::sort(key.begin(), key.end());
-        std::vector<int> order((size_t)pc);
-        for (long q = 0; q < pc; ++q)
-            order[(size_t)q] = (int)(key[(size_t)q] & 0xFFFFFFFFll);
-        GC_TRY(p->pair_order.alloc((size_t)pc));
-        GC_TRY_CUDA(cudaMemcpy(p->pair_order.p, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
+        const gc::host::WalkConfig cfg = gc::host::walk_config(nframes, k);
+        GC_TRY(p->ft.create(natoms, nframes, k, pb, pc, o.pair_list, p->pair_ab.p,
+                            gc::host::ksg_block_queries(natoms, nframes, 8.0 * (1 << 30)), cfg.pair_tile));
+        std::vector<std::vector<gc::WalkParams>> waves;
+        for (int b = 0; b < p->ft.blocks(); ++b)
+            waves.push_back({p->ft.desc(p->X.p, p->cnt.p, p->status.p, b)});
+        GC_TRY(p->fl.build(waves, {p->ft.desc(p->X.p, p->cnt.p, p->status.p, 0)}, cfg));
     }
     *out = p.release();
     return GC_OK;
@@ -249,63 +208,10 @@ gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi
         GC_TRY_CUDA(cudaEventRecord(p->ev0, s));
         if (p->fast)
         {
-            const int T = p->T;
-            GC_TRY_CUDA(gc::launch_ksg_x32(p->X.p, p->natoms, T, p->X32.p, p->eps.p, s));
-            GC_TRY_CUDA(cudaMemsetAsync(p->reasons.p, 0, 8 * sizeof(unsigned), s));
-            GC_TRY_CUDA(cudaMemsetAsync(p->walk_elems.p, 0, sizeof(unsigned long long), s));
-            GC_TRY_CUDA(cudaMemsetAsync(p->hq_len.p, 0, sizeof(unsigned), s));
-            p->launches += 1;
-            gc::WalkParams w{};
-            w.X32          = p->X32.p;
-            w.X64          = p->X.p;
-            w.eps_atom     = p->eps.p;
-            w.S            = p->S.p;
-            w.P            = p->P.p;
-            w.Lpad         = p->Lpad;
-            w.Qp           = p->Qp;
-            w.T            = T;
-            w.K            = p->K;
-            w.box          = gc::ksg_box_count(T, p->K);
-            w.pair_begin   = p->pair_begin;
-            w.pair_count   = p->pair_count;
-            w.pair_ab      = p->pair_ab.p;
-            w.pair_order   = p->pair_order.p;
-            w.shift        = p->shift;
-            w.wres         = p->wres.p;
-            w.hq           = p->hq.p;
-            w.hq_len       = p->hq_len.p;
-            w.hq_cap       = p->hq_cap;
-            w.cnt          = p->cnt.p;
-            w.task_counter = p->task_counter.p;
-            w.status       = p->status.p;
-            w.walk_elems   = p->walk_elems.p;
-            w.reasons      = p->reasons.p;
-            for (int i0 = 0; i0 < T; i0 += p->Q)
-            {
-                const int Qb = T - i0 < p->Q ? T - i0 : p->Q;
-                GC_TRY_CUDA(gc::launch_ksg_rows(p->X32.p, p->natoms, T, i0, Qb, p->Qp, p->Lpad, p->S.p, p->P.p, s));
-                GC_TRY_CUDA(cudaMemsetAsync(p->task_counter.p, 0, 2 * sizeof(unsigned long long), s));
-                w.i0 = i0;
-                w.Q  = Qb;
-                GC_TRY_CUDA(gc::launch_ksg_walk(w, p->sms, s));
-                GC_TRY_CUDA(gc::launch_ksg_finish(w, p->sms, s));
-                p->launches += 3;
-            }
-            gc::FixupParams fp{};
-            fp.X64        = p->X.p;
-            fp.T          = T;
-            fp.K          = p->K;
-            fp.box        = w.box;
-            fp.rank_shift = gc::rank_top_shift(w.box, T);
-            fp.pair_begin = p->pair_begin;
-            fp.pair_count = p->pair_count;
-            fp.pair_ab    = p->pair_ab.p;
-            fp.cnt        = p->cnt.p;
-            fp.hq         = p->hq.p;
-            fp.hq_len     = p->hq_len.p;
-            fp.hq_cap     = p->hq_cap;
-            GC_TRY_CUDA(gc::launch_ksg_fixup(fp, p->sms, s));
-            p->launches += 2;
+            GC_TRY_CUDA(gc::launch_ksg_x32(p->X.p, p->natoms, p->T, p->ft.X32.p, p->ft.eps.p, s));
+            GC_TRY(p->ft.clear(s));
+            GC_TRY(p->fl.enqueue(p->sms, s));
+            p->launches += 1 + p->fl.launches;
         }
         else
         {
@@ -334,10 +240,10 @@ gc_status gc_ksg_plan_sync(gc_ksg_plan* p)
     if (p->fast)
     {
         unsigned long long we = 0;
-        GC_TRY_CUDA(cudaMemcpy(&we, p->walk_elems.p, sizeof(we), cudaMemcpyDeviceToHost));
+        GC_TRY_CUDA(cudaMemcpy(&we, p->ft.walk_elems.p, sizeof(we), cudaMemcpyDeviceToHost));
         p->walk_mean = (double)we / ((double)p->pair_count * p->T);
         unsigned rc[8] = {};
-        GC_TRY_CUDA(cudaMemcpy(rc, p->reasons.p, sizeof(rc), cudaMemcpyDeviceToHost));
+        GC_TRY_CUDA(cudaMemcpy(rc, p->ft.reasons.p, sizeof(rc), cudaMemcpyDeviceToHost));
         for (int r = 0; r < 8; ++r)
         {
             p->reason_counts[r] = (long)rc[r];
@@ -388,18 +294,6 @@ void gc_ksg_plan_destroy(gc_ksg_plan* p)
             cudaEventDestroy(p->ev0);
         if (p->ev1)
             cudaEventDestroy(p->ev1);
-        p->X.reset();
-        p->psi.reset();
-        p->cnt.reset();
-        p->status.reset();
-        p->pair_ab.reset();
-        p->X32.reset();
-        p->eps.reset();
-        p->S.reset();
-        p->P.reset();
-        p->task_counter.reset();
-        p->walk_elems.reset();
-        p->reasons.reset();
         delete p; // the remaining buffers are freed with this device current
     }
 }

@@ -1,0 +1,337 @@
+// KSG matrices of many trajectories in one batched run (no counterpart in
+// the reference, which runs kraskov_corrmatrix once per trajectory,
+// lib/correlation_core.cpp:324-459).
+//
+// Every trajectory gets the single-trajectory plan's workspace; the query
+// blocks of all trajectories then run together: each wave is one launch of
+// the row sort, the walk and the finish whose tasks are drawn from every
+// trajectory still active (a global task counter over a prefix table of
+// per-trajectory descriptors), so trajectories of uneven atom and frame
+// counts and different k share the GPU.  The whole sequence (normalisation,
+// FP32 rows, waves, exact fix-up, MI reduction) is captured once into a CUDA
+// graph and replayed; the walk's launch shape (warps per CTA, atom-tile size
+// of the pair order) is chosen by timing the candidates on the first wave the
+// first time a shape class is seen.
+
+#include "gc_geom.h"
+#include "gc_internal.h"
+#include "host_common.h"
+#include "ksg_host.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using namespace gc::host;
+
+namespace {
+
+constexpr double kBatchBudget = 24.0 * (1ull << 30); // sorted rows of one wave, all trajectories
+
+struct BatchTraj
+{
+    int                 natoms = 0, T = 0, K = 0;
+    long                pairs  = 0;
+    DevBuf<double>      xyz, X, psi, mi;
+    DevBuf<uint32_t>    cnt;
+    KsgTraj             ft;
+    std::vector<double> host_mi;
+};
+
+struct BatchPlan
+{
+    int                                     device = 0, sms = 148;
+    std::vector<std::unique_ptr<BatchTraj>> t;
+    DevBuf<int>                             status;
+    KsgLaunch                               fl;
+    WalkConfig                              cfg;
+    bool                                    tuned  = false;
+    cudaStream_t                            stream = nullptr;
+    cudaGraphExec_t                         exec   = nullptr;
+    std::vector<int>                        key; // natoms, T, k per trajectory
+    ~BatchPlan()
+    {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        if (stream)
+            cudaStreamDestroy(stream);
+    }
+};
+
+std::mutex                 g_batch_mutex;
+std::unique_ptr<BatchPlan> g_batch[64];
+
+// Query-block size of every trajectory for the smallest number of waves
+// whose sorted rows fit the budget.
+std::vector<int> batch_blocks(const std::vector<std::unique_ptr<BatchTraj>>& t)
+{
+    int maxT = 0;
+    for (const auto& b : t)
+        maxT = std::max(maxT, b->T);
+    for (int waves = 1;; ++waves)
+    {
+        std::vector<int> q;
+        double           bytes = 0.0;
+        for (const auto& b : t)
+        {
+            int Qb = ((b->T + waves - 1) / waves + 31) & ~31;
+            Qb     = std::min(Qb, b->T);
+            q.push_back(Qb);
+            bytes += (double)b->natoms * (((b->T - 1) + 31) & ~31) * ((Qb + 31) & ~31) * 6.0;
+        }
+        if (bytes <= kBatchBudget || waves >= maxT)
+            return q;
+    }
+}
+
+gc_status build_launch(BatchPlan& bp, const WalkConfig& cfg)
+{
+    int nw = 0;
+    for (const auto& b : bp.t)
+        nw = std::max(nw, b->ft.blocks());
+    std::vector<std::vector<gc::WalkParams>> waves((size_t)nw);
+    std::vector<gc::WalkParams>              traj;
+    for (size_t i = 0; i < bp.t.size(); ++i)
+    {
+        BatchTraj& b = *bp.t[i];
+        GC_TRY(b.ft.set_pair_tile(cfg.pair_tile));
+        for (int w = 0; w < b.ft.blocks(); ++w)
+            waves[(size_t)w].push_back(b.ft.desc(b.X.p, b.cnt.p, bp.status.p + i, w));
+        traj.push_back(b.ft.desc(b.X.p, b.cnt.p, bp.status.p + i, 0));
+    }
+    return bp.fl.build(waves, traj, cfg);
+}
+
+// Everything after the input upload, in stream order (graph-capturable).
+gc_status enqueue_all(BatchPlan& bp, cudaStream_t s)
+{
+    GC_TRY_CUDA(cudaMemsetAsync(bp.status.p, 0, sizeof(int) * bp.t.size(), s));
+    for (size_t i = 0; i < bp.t.size(); ++i)
+    {
+        BatchTraj& b = *bp.t[i];
+        gc::launch_ksg_prepare(b.xyz.p, b.natoms, b.T, b.X.p, bp.status.p + i, s);
+        GC_TRY_CUDA(gc::launch_ksg_x32(b.X.p, b.natoms, b.T, b.ft.X32.p, b.ft.eps.p, s));
+        GC_TRY(b.ft.clear(s));
+    }
+    GC_TRY(bp.fl.enqueue(bp.sms, s));
+    for (auto& b : bp.t)
+        gc::launch_ksg_finalize(b->cnt.p, b->pairs, b->T, b->K, b->psi.p, b->mi.p, s);
+    GC_TRY_CUDA(cudaGetLastError());
+    return GC_OK;
+}
+
+// Times each candidate walk configuration on the first wave and keeps the
+// fastest (inputs must be uploaded; the status words are ignored here).
+gc_status autotune(BatchPlan& bp)
+{
+    cudaStream_t s = bp.stream;
+    for (size_t i = 0; i < bp.t.size(); ++i)
+    {
+        BatchTraj& b = *bp.t[i];
+        gc::launch_ksg_prepare(b.xyz.p, b.natoms, b.T, b.X.p, bp.status.p + i, s);
+        GC_TRY_CUDA(gc::launch_ksg_x32(b.X.p, b.natoms, b.T, b.ft.X32.p, b.ft.eps.p, s));
+    }
+    int maxT = 0, maxK = 0;
+    for (const auto& b : bp.t)
+    {
+        maxT = std::max(maxT, b->T);
+        maxK = std::max(maxK, b->K);
+    }
+    cudaEvent_t e0, e1;
+    GC_TRY_CUDA(cudaEventCreate(&e0));
+    GC_TRY_CUDA(cudaEventCreate(&e1));
+    float      best = 1e30f;
+    WalkConfig best_cfg;
+    gc_status  st = GC_OK;
+    for (const WalkConfig& c : walk_candidates(maxT))
+    {
+        if ((st = build_launch(bp, c)) != GC_OK)
+            break;
+        float ms = 0.0f;
+        for (int rep = 0; rep < 2 && st == GC_OK; ++rep) // the first run warms up
+        {
+            for (auto& b : bp.t)
+                if ((st = b->ft.clear(s)) != GC_OK)
+                    break;
+            cudaEventRecord(e0, s);
+            if (st == GC_OK)
+                st = bp.fl.enqueue(bp.sms, s, 0, 0, false);
+            cudaEventRecord(e1, s);
+            if (cudaEventSynchronize(e1) != cudaSuccess)
+                st = fail(GC_ERR_CUDA, "autotune run failed");
+            cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (st != GC_OK)
+            break;
+        if (ms < best)
+        {
+            best     = ms;
+            best_cfg = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    GC_TRY(st);
+    remember_walk_config(maxT, maxK, best_cfg);
+    bp.cfg   = best_cfg;
+    bp.tuned = true;
+    return build_launch(bp, best_cfg);
+}
+
+gc_status create_plan(const gc_traj_view* trajs, const int* ks, int ntraj, int device, std::unique_ptr<BatchPlan>& out)
+{
+    auto bp    = std::make_unique<BatchPlan>();
+    bp->device = device;
+    GC_TRY_CUDA(cudaDeviceGetAttribute(&bp->sms, cudaDevAttrMultiProcessorCount, device));
+    GC_TRY_CUDA(cudaStreamCreateWithFlags(&bp->stream, cudaStreamNonBlocking));
+    GC_TRY(bp->status.alloc((size_t)ntraj));
+    int maxT = 0, maxK = 0;
+    for (int i = 0; i < ntraj; ++i)
+    {
+        auto b    = std::make_unique<BatchTraj>();
+        b->natoms = trajs[i].natoms;
+        b->T      = trajs[i].nframes;
+        b->K      = ks[i];
+        b->pairs  = (long)b->natoms * (b->natoms - 1) / 2;
+        maxT      = std::max(maxT, b->T);
+        maxK      = std::max(maxK, b->K);
+        GC_TRY(b->xyz.alloc((size_t)b->natoms * b->T * 3));
+        GC_TRY(b->X.alloc((size_t)b->natoms * b->T * 3));
+        GC_TRY(b->psi.alloc((size_t)b->T + 1));
+        GC_TRY(b->mi.alloc((size_t)b->pairs));
+        GC_TRY(b->cnt.alloc((size_t)b->T * b->pairs));
+        const std::vector<double> psi = digamma_table(b->T);
+        GC_TRY_CUDA(cudaMemcpy(b->psi.p, psi.data(), sizeof(double) * psi.size(), cudaMemcpyHostToDevice));
+        bp->key.insert(bp->key.end(), {b->natoms, b->T, b->K});
+        bp->t.push_back(std::move(b));
+    }
+    const std::vector<int> q = batch_blocks(bp->t);
+    bp->cfg                  = walk_config(maxT, maxK);
+    for (size_t i = 0; i < bp->t.size(); ++i)
+    {
+        BatchTraj& b = *bp->t[i];
+        GC_TRY(b.ft.create(b.natoms, b.T, b.K, 0, b.pairs, nullptr, nullptr, q[i], bp->cfg.pair_tile));
+    }
+    GC_TRY(build_launch(*bp, bp->cfg));
+    out = std::move(bp);
+    return GC_OK;
+}
+
+gc_status capture(BatchPlan& bp)
+{
+    if (bp.exec)
+    {
+        cudaGraphExecDestroy(bp.exec);
+        bp.exec = nullptr;
+    }
+    cudaGraph_t graph = nullptr;
+    GC_TRY_CUDA(cudaStreamBeginCapture(bp.stream, cudaStreamCaptureModeThreadLocal));
+    const gc_status   st = enqueue_all(bp, bp.stream);
+    const cudaError_t ce = cudaStreamEndCapture(bp.stream, &graph);
+    if (st != GC_OK)
+    {
+        if (graph)
+            cudaGraphDestroy(graph);
+        return st;
+    }
+    GC_TRY_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&bp.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    GC_TRY_CUDA(ie);
+    return GC_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+gc_status gc_ksg_batch(const gc_traj_view* trajs, const int* ks, int ntraj, const gc_opts* opts, double* const* mi)
+{
+    if (!trajs || !ks || !mi || ntraj < 1)
+        return fail(GC_ERR_INVALID, "gc_ksg_batch: need trajectories, k values and output matrices");
+    const gc_opts o = opts ? *opts : defaults();
+    for (int i = 0; i < ntraj; ++i)
+    {
+        GC_TRY(check_view(&trajs[i]));
+        if (!mi[i])
+            return fail(GC_ERR_INVALID, "gc_ksg_batch: null output matrix");
+        const int n = trajs[i].natoms, T = trajs[i].nframes, k = ks[i];
+        if (n < 2 || k < 1 || T <= k)
+            return fail(GC_ERR_INVALID, "gc_ksg_batch: every trajectory needs >= 2 atoms and nframes > k >= 1");
+        if (T - 1 > 16384)
+            return fail(GC_ERR_INVALID, "gc_ksg_batch: nframes <= 16385 (use gc_ksg_matrix for longer trajectories)");
+    }
+    DeviceScope dev(o.device);
+    GC_TRY(dev.st);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur < 0 || cur >= 64)
+        return fail(GC_ERR_INVALID, "gc_ksg_batch: device ordinal beyond the batch cache");
+    std::vector<int> key;
+    for (int i = 0; i < ntraj; ++i)
+        key.insert(key.end(), {trajs[i].natoms, trajs[i].nframes, ks[i]});
+
+    std::lock_guard<std::mutex> lock(g_batch_mutex); // one batch per process at a time
+    std::unique_ptr<BatchPlan>& bp = g_batch[cur];
+    if (!bp || bp->key != key)
+    {
+        bp.reset();
+        GC_TRY(create_plan(trajs, ks, ntraj, cur, bp));
+    }
+    cudaStream_t s = bp->stream;
+    for (int i = 0; i < ntraj; ++i)
+        GC_TRY(upload_traj(&trajs[i], bp->t[(size_t)i]->xyz.p, s));
+    if (!bp->tuned)
+    {
+        GC_TRY(autotune(*bp));
+        GC_TRY(capture(*bp));
+    }
+    else if (!bp->exec)
+        GC_TRY(capture(*bp));
+    GC_TRY_CUDA(cudaGraphLaunch(bp->exec, s));
+    std::vector<int> st((size_t)ntraj);
+    GC_TRY_CUDA(cudaMemcpyAsync(st.data(), bp->status.p, sizeof(int) * ntraj, cudaMemcpyDeviceToHost, s));
+    for (auto& b : bp->t)
+    {
+        b->host_mi.resize((size_t)b->pairs);
+        GC_TRY_CUDA(cudaMemcpyAsync(b->host_mi.data(), b->mi.p, sizeof(double) * b->pairs, cudaMemcpyDeviceToHost, s));
+    }
+    GC_TRY_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < ntraj; ++i)
+        GC_TRY(status_to_error(st[(size_t)i] & ~gc::kStatFallback));
+    for (int i = 0; i < ntraj; ++i)
+    {
+        const BatchTraj& b = *bp->t[(size_t)i];
+        double*          m = mi[i];
+        const int        n = b.natoms;
+        std::memset(m, 0, sizeof(double) * (size_t)n * n);
+        for (int a = 0; a < n; ++a)
+            m[(size_t)a * n + a] = 2000.0;
+        for (long p = 0; p < b.pairs; ++p)
+        {
+            int a1, a2;
+            gc::pair_from_index(p, &a1, &a2);
+            m[(size_t)a1 * n + a2] = b.host_mi[(size_t)p];
+            m[(size_t)a2 * n + a1] = b.host_mi[(size_t)p];
+        }
+    }
+    return GC_OK;
+}
+
+void gc_ksg_batch_release(void)
+{
+    std::lock_guard<std::mutex> lock(g_batch_mutex);
+    for (auto& b : g_batch)
+        if (b)
+        {
+            DeviceScope dev(b->device);
+            b.reset();
+        }
+}
+
+} // extern "C"

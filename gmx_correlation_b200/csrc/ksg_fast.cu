@@ -84,6 +84,21 @@ __global__ void ksg_x32_kernel(const double* __restrict__ X64, int natoms, int T
     }
 }
 
+// The descriptor owning task t: the largest d with prefix[d] <= t.
+__device__ __forceinline__ int batch_desc(const long long* __restrict__ prefix, int n, long long t)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= t)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
 // One CTA per (atom, query): the row's T-1 marginal distances (self
 // excluded), sorted ascending with their frames.  Keys are
 // (distance bits << 32 | frame).  A bucket pass over the row's own
@@ -95,25 +110,36 @@ __global__ void ksg_x32_kernel(const double* __restrict__ X64, int natoms, int T
 // are sorted by a bitonic network instead.
 constexpr int kRowsThreads = 256;
 
-__global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(const float4* __restrict__ X32, int T, int i0, int Q,
-                                                                int Qp, int Lpad, int N2, int nbin,
-                                                                float* __restrict__ S, uint16_t* __restrict__ P)
+__global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
 {
     extern __shared__ __align__(16) unsigned char rows_smem[];
-    unsigned long long* keys   = reinterpret_cast<unsigned long long*>(rows_smem); // [N2] sorted output
-    unsigned*           hist   = reinterpret_cast<unsigned*>(keys + N2);           // [nbin]
-    unsigned*           cursor = hist + nbin;                                      // [nbin]
     __shared__ unsigned red_min[kRowsThreads / 32], red_max[kRowsThreads / 32];
     __shared__ unsigned coarse[kRowsThreads / 32][64];
     __shared__ float    cum[65];
     __shared__ int      crowded;
 
-    const int     row = blockIdx.x;
-    const int     a   = row / Q;
-    const int     iq  = row - a * Q;
-    const int     i   = i0 + iq;
-    const int     N   = T - 1;
-    const int     tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // row blockIdx.x of the launch -> descriptor, atom, query of its block
+    const long long   r   = blockIdx.x;
+    const int         dsc = batch_desc(B.rprefix, B.n, r);
+    const WalkParams& w   = B.d[dsc];
+    const int         T = w.T, Q = w.Q, Qp = w.Qp, Lpad = w.Lpad;
+    const int         row = (int)(r - B.rprefix[dsc]);
+    const int         a   = row / Q;
+    const int         iq  = row - a * Q;
+    const int         i   = w.i0 + iq;
+    const int         N   = T - 1;
+    const int         tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int               N2  = 256;
+    while (N2 < N)
+        N2 <<= 1;
+    // bucket pass up to 8192 keys; longer rows use the bitonic network alone
+    const int           nbin   = N2 <= 8192 ? (N2 < 4096 ? N2 : 4096) : 0;
+    unsigned long long* keys   = reinterpret_cast<unsigned long long*>(rows_smem); // [N2] sorted output
+    unsigned*           hist   = reinterpret_cast<unsigned*>(keys + N2);           // [nbin]
+    unsigned*           cursor = hist + nbin;                                      // [nbin]
+    float*              S      = w.S;
+    uint16_t*           P      = w.P;
+    const float4*       X32    = w.X32;
     const float4* xr  = X32 + (size_t)a * T;
     const float4  q   = xr[i];
     auto          frame_of = [i](int m) { return m < i ? m : m + 1; };
@@ -443,18 +469,9 @@ struct Task
     int  a1, a2;
 };
 
-__device__ __forceinline__ bool next_task(const WalkParams& p, unsigned long long* counter, long long total,
-                                          long long* s_task, Task& tk)
+__device__ __forceinline__ void task_pair(const WalkParams& p, long k, Task& tk)
 {
-    if (threadIdx.x == 0)
-        *s_task = (long long)atomicAdd(counter, 1ull);
-    __syncthreads();
-    const long long t = *s_task;
-    if (t >= total)
-        return false;
-    tk.c         = (int)(t / p.pair_count);
-    const long k = (long)(t - (long long)tk.c * p.pair_count);
-    tk.pl        = p.pair_order ? (long)p.pair_order[k] : k;
+    tk.pl = p.pair_order ? (long)p.pair_order[k] : k;
     if (p.pair_ab)
     {
         tk.a1 = p.pair_ab[tk.pl].x;
@@ -462,6 +479,27 @@ __device__ __forceinline__ bool next_task(const WalkParams& p, unsigned long lon
     }
     else
         pair_from_index(p.pair_begin + tk.pl, &tk.a1, &tk.a2);
+}
+
+__device__ __forceinline__ bool next_task(const WalkBatch& B, long long total, long long* s_task, int* s_desc,
+                                          Task& tk, int& d)
+{
+    if (threadIdx.x == 0)
+    {
+        const long long t = (long long)atomicAdd(B.counter, 1ull);
+        *s_task           = t;
+        if (t < total)
+            *s_desc = batch_desc(B.wprefix, B.n, t);
+    }
+    __syncthreads();
+    const long long t = *s_task;
+    if (t >= total)
+        return false;
+    d                   = *s_desc;
+    const WalkParams& p = B.d[d];
+    const long long   lt = t - B.wprefix[d];
+    tk.c                 = (int)(lt / p.pair_count);
+    task_pair(p, (long)(lt - (long long)tk.c * p.pair_count), tk);
     return true;
 }
 
@@ -478,25 +516,28 @@ __device__ __forceinline__ unsigned long long pack_walk(int bstar, int prefix, i
 // Pass 1: walk the sorted row, histogram v = max(s, d) per lane.  STAGED:
 // the pair's coordinate rows are copied into shared memory per task.
 template <bool STAGED>
-__global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkParams p)
+__global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ long long s_task;
+    __shared__ int       s_desc;
     const int            warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
     float4*              sx   = reinterpret_cast<float4*>(smem_raw);
-    unsigned char*       base = smem_raw + (STAGED ? (size_t)2 * p.T * 16 : 0) + (size_t)warp * kWalkBuckets * 32;
+    unsigned char*       base = smem_raw + (STAGED ? (size_t)2 * B.maxT * 16 : 0) + (size_t)warp * kWalkBuckets * 32;
     // bucket b of this lane: byte b % 4 of word (b / 4) * 32 + lane, so the
     // 32 lanes of a warp always hit 32 different banks
     uint8_t* hist = base + lane * 4;
     auto     H    = [hist](unsigned b) -> uint8_t& { return hist[(b >> 2) * 128 + (b & 3)]; };
 
-    const int       T = p.T, K = p.K, Llen = T - 1, shift = p.shift;
-    const int       ngroups = (p.Q + 31) >> 5;
-    const long long total   = (long long)((ngroups + warps - 1) / warps) * p.pair_count;
-    const float     inf     = __int_as_float(0x7f800000);
+    const long long total = B.wprefix[B.n];
+    const float     inf   = __int_as_float(0x7f800000);
     Task            tk;
-    while (next_task(p, p.task_counter, total, &s_task, tk))
+    int             dsc;
+    while (next_task(B, total, &s_task, &s_desc, tk, dsc))
     {
+        const WalkParams& p       = B.d[dsc];
+        const int         T       = p.T, K = p.K, Llen = T - 1, shift = p.shift;
+        const int         ngroups = (p.Q + 31) >> 5;
         const float4* xa = p.X32 + (size_t)tk.a1 * T;
         const float4* xb = p.X32 + (size_t)tk.a2 * T;
         if (STAGED)
@@ -632,7 +673,7 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkParams p)
 }
 
 // Pass 2: from the walk's k-th bucket to n_x, n_y (or a hand-over).
-__global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkParams p)
+__global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBatch B)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int      warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -646,29 +687,29 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkPa
     int*      bp = reinterpret_cast<int*>(bd + kBandCap * 32);
     uint16_t* bj = reinterpret_cast<uint16_t*>(reinterpret_cast<float*>(base) + 4 * kBandCap * 32) + lane;
 
-    const int       T = p.T, K = p.K, Llen = T - 1, shift = p.shift;
-    const long long total = (long long)((p.Q + 31) >> 5) * p.pair_count;
-    const ScanGrid  grid(p.box);
+    const long long total = B.fprefix[B.n];
     for (;;)
     {
         // warp task: query group g outer, pairs (in tile order) inner
-        long long t = 0;
+        long long t   = 0;
+        int       dsc = 0;
         if (lane == 0)
-            t = (long long)atomicAdd(p.task_counter + 1, 1ull);
-        t = __shfl_sync(kFull, t, 0);
+        {
+            t = (long long)atomicAdd(B.counter + 1, 1ull);
+            if (t < total)
+                dsc = batch_desc(B.fprefix, B.n, t);
+        }
+        t   = __shfl_sync(kFull, t, 0);
+        dsc = __shfl_sync(kFull, dsc, 0);
         if (t >= total)
             break;
-        Task tk;
-        const int  g = (int)(t / p.pair_count);
-        const long k = (long)(t - (long long)g * p.pair_count);
-        tk.pl        = p.pair_order ? (long)p.pair_order[k] : k;
-        if (p.pair_ab)
-        {
-            tk.a1 = p.pair_ab[tk.pl].x;
-            tk.a2 = p.pair_ab[tk.pl].y;
-        }
-        else
-            pair_from_index(p.pair_begin + tk.pl, &tk.a1, &tk.a2);
+        const WalkParams& p  = B.d[dsc];
+        const int         T  = p.T, K = p.K, Llen = T - 1, shift = p.shift;
+        const ScanGrid    grid(p.box);
+        const long long   lt = t - B.fprefix[dsc];
+        Task              tk;
+        const int         g = (int)(lt / p.pair_count);
+        task_pair(p, (long)(lt - (long long)g * p.pair_count), tk);
         const float4* xa   = p.X32 + (size_t)tk.a1 * T;
         const float4* xb   = p.X32 + (size_t)tk.a2 * T;
         const int     iq   = g * 32 + lane;
@@ -1024,7 +1065,7 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkPa
 }
 
 // Exact FP64 statistics of one handed-over (query, pair): cnt index idx.
-__device__ __forceinline__ void fixup_one(const FixupParams& p, long long idx, unsigned* hist, int lane)
+__device__ __forceinline__ void fixup_one(const WalkParams& p, long long idx, unsigned* hist, int lane)
 {
     const int  i  = (int)(idx / p.pair_count);
     const long pl = (long)(idx - (long long)i * p.pair_count);
@@ -1042,31 +1083,41 @@ __device__ __forceinline__ void fixup_one(const FixupParams& p, long long idx, u
     __syncwarp();
 }
 
-// The queued hand-overs, one warp each, spread over the whole grid.
-__global__ void __launch_bounds__(256) ksg_fixup_queue_kernel(FixupParams p)
+// The queued hand-overs of every descriptor, one warp each, spread over the grid.
+__global__ void __launch_bounds__(256) ksg_fixup_queue_kernel(WalkBatch B)
 {
     __shared__ unsigned hist[8][256];
-    const int      warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const unsigned n    = min(*p.hq_len, p.hq_cap);
-    for (unsigned e = blockIdx.x * 8 + warp; e < n; e += gridDim.x * 8)
-        fixup_one(p, (long long)p.hq[e], hist[warp], lane);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int d = 0; d < B.n; ++d)
+    {
+        const WalkParams& p = B.d[d];
+        if (!p.hq)
+            continue;
+        const unsigned n = min(*p.hq_len, p.hq_cap);
+        for (unsigned e = blockIdx.x * 8 + warp; e < n; e += gridDim.x * 8)
+            fixup_one(p, (long long)p.hq[e], hist[warp], lane);
+    }
 }
 
-// Any kHandOver mark left (the queue overflowed, or no queue): scan cnt.
-__global__ void __launch_bounds__(256) ksg_fixup_kernel(FixupParams p)
+// Any kHandOver mark left (a queue overflowed): scan the counts.
+__global__ void __launch_bounds__(256) ksg_fixup_kernel(WalkBatch B)
 {
     __shared__ unsigned hist[8][256];
-    const int       warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long n    = (long long)p.T * p.pair_count;
-    for (long long c0 = ((long long)blockIdx.x * 8 + warp) * 32; c0 < n; c0 += (long long)gridDim.x * 8 * 32)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int d = 0; d < B.n; ++d)
     {
-        const long long e  = c0 + lane;
-        unsigned        hm = __ballot_sync(kFull, e < n && p.cnt[e] == kHandOver);
-        while (hm)
+        const WalkParams& p = B.d[d];
+        const long long   n = (long long)p.T * p.pair_count;
+        for (long long c0 = ((long long)blockIdx.x * 8 + warp) * 32; c0 < n; c0 += (long long)gridDim.x * 8 * 32)
         {
-            const int src = __ffs(hm) - 1;
-            hm &= hm - 1;
-            fixup_one(p, c0 + src, hist[warp], lane);
+            const long long e  = c0 + lane;
+            unsigned        hm = __ballot_sync(kFull, e < n && p.cnt[e] == kHandOver);
+            while (hm)
+            {
+                const int src = __ffs(hm) - 1;
+                hm &= hm - 1;
+                fixup_one(p, c0 + src, hist[warp], lane);
+            }
         }
     }
 }
@@ -1077,14 +1128,13 @@ cudaError_t launch_ksg_x32(const double* X64, int natoms, int T, float4* X32, fl
     return cudaGetLastError();
 }
 
-cudaError_t launch_ksg_rows(const float4* X32, int natoms, int T, int i0, int Q, int Qp, int Lpad, float* S,
-                            uint16_t* P, cudaStream_t s)
+cudaError_t launch_ksg_rows(const WalkBatch& b, long long rows, cudaStream_t s)
 {
+    if (rows <= 0)
+        return cudaSuccess;
     int N2 = 256;
-    while (N2 < T - 1)
+    while (N2 < b.maxT - 1)
         N2 <<= 1;
-    // bucket pass up to 8192 keys (keys + bins); longer rows use the bitonic
-    // network alone
     const int    nbin = N2 <= 8192 ? (N2 < 4096 ? N2 : 4096) : 0;
     const size_t smem = (size_t)N2 * 8 + (size_t)nbin * 8;
     // static shared memory comes on top of the dynamic part: always raise
@@ -1092,7 +1142,7 @@ cudaError_t launch_ksg_rows(const float4* X32, int natoms, int T, int i0, int Q,
     cudaError_t e = cudaFuncSetAttribute(ksg_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;
-    ksg_rows_kernel<<<(unsigned)((long)natoms * Q), kRowsThreads, smem, s>>>(X32, T, i0, Q, Qp, Lpad, N2, nbin, S, P);
+    ksg_rows_kernel<<<(unsigned)rows, kRowsThreads, smem, s>>>(b);
     return cudaGetLastError();
 }
 
@@ -1100,26 +1150,27 @@ cudaError_t launch_ksg_rows(const float4* X32, int natoms, int T, int i0, int Q,
 // room for the static variables).
 constexpr size_t kSmemBudget = 226 * 1024;
 
-// Warps per CTA that fit the budget next to the staged coordinate rows, or 0.
-static int fit_warps(int T, size_t per_warp, int max_warps, int min_warps)
+int walk_max_staged_warps(int maxT)
 {
-    const size_t rows = (size_t)2 * T * 16;
+    const size_t rows = (size_t)2 * maxT * 16;
     if (rows >= kSmemBudget)
         return 0;
-    int w = (int)((kSmemBudget - rows) / per_warp);
-    w     = w > max_warps ? max_warps : w;
-    return w >= min_warps ? w : 0;
+    int w = (int)((kSmemBudget - rows) / ((size_t)kWalkBuckets * 32));
+    w     = w > kWalkWarps ? kWalkWarps : w;
+    return w >= 8 ? w : 0;
 }
 
-static cudaError_t launch_tasks(void (*kernel)(WalkParams), int max_warps, size_t per_warp, int sms, WalkParams p,
-                                cudaStream_t s)
+void walk_shape(int maxT, int* warps, bool* staged)
 {
-    // stage the pair's coordinate rows in shared memory when enough warps fit
-    int warps = fit_warps(p.T, per_warp, max_warps, 8);
-    p.staged  = warps > 0 ? 1 : 0;
-    if (!p.staged)
-        warps = max_warps;
-    const size_t smem = (p.staged ? (size_t)2 * p.T * 16 : 0) + (size_t)warps * per_warp;
+    const int w = walk_max_staged_warps(maxT);
+    *staged     = w > 0;
+    *warps      = w > 0 ? w : kWalkWarps;
+}
+
+cudaError_t launch_ksg_walk(const WalkBatch& b, int warps, bool staged, int sms, cudaStream_t s)
+{
+    void (*kernel)(WalkBatch) = staged ? ksg_walk_kernel<true> : ksg_walk_kernel<false>;
+    const size_t smem = (staged ? (size_t)2 * b.maxT * 16 : 0) + (size_t)warps * kWalkBuckets * 32;
     cudaError_t  e    = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;
@@ -1128,18 +1179,11 @@ static cudaError_t launch_tasks(void (*kernel)(WalkParams), int max_warps, size_
     if (e != cudaSuccess)
         return e;
     per_sm = per_sm < 1 ? 1 : per_sm;
-    kernel<<<sms * per_sm, warps * 32, smem, s>>>(p);
+    kernel<<<sms * per_sm, warps * 32, smem, s>>>(b);
     return cudaGetLastError();
 }
 
-cudaError_t launch_ksg_walk(const WalkParams& p, int sms, cudaStream_t s)
-{
-    const bool staged = fit_warps(p.T, (size_t)kWalkBuckets * 32, kWalkWarps, 8) > 0;
-    return launch_tasks(staged ? ksg_walk_kernel<true> : ksg_walk_kernel<false>, kWalkWarps,
-                        (size_t)kWalkBuckets * 32, sms, p, s);
-}
-
-cudaError_t launch_ksg_finish(const WalkParams& p, int sms, cudaStream_t s)
+cudaError_t launch_ksg_finish(const WalkBatch& b, int sms, cudaStream_t s)
 {
     const size_t smem = (size_t)kFinishWarps * kBandSlotBytes * kBandCap * 32;
     cudaError_t  e    = cudaFuncSetAttribute(ksg_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1150,20 +1194,17 @@ cudaError_t launch_ksg_finish(const WalkParams& p, int sms, cudaStream_t s)
     if (e != cudaSuccess)
         return e;
     per_sm = per_sm < 1 ? 1 : per_sm;
-    ksg_finish_kernel<<<sms * per_sm, kFinishWarps * 32, smem, s>>>(p);
+    ksg_finish_kernel<<<sms * per_sm, kFinishWarps * 32, smem, s>>>(b);
     return cudaGetLastError();
 }
 
-cudaError_t launch_ksg_fixup(const FixupParams& p, int sms, cudaStream_t s)
+cudaError_t launch_ksg_fixup(const WalkBatch& b, int sms, cudaStream_t s)
 {
-    if (p.hq)
-    {
-        ksg_fixup_queue_kernel<<<sms * 4, 256, 0, s>>>(p);
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess)
-            return e;
-    }
-    ksg_fixup_kernel<<<sms * 4, 256, 0, s>>>(p);
+    ksg_fixup_queue_kernel<<<sms * 4, 256, 0, s>>>(b);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return e;
+    ksg_fixup_kernel<<<sms * 4, 256, 0, s>>>(b);
     return cudaGetLastError();
 }
 

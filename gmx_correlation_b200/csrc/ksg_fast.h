@@ -22,35 +22,35 @@ struct WalkParams
     const float4*   X32;      // [natoms][T] centred FP32 coordinates
     const double*   X64;      // [3*natoms][T] normalised rows (reference arithmetic)
     const float*    eps_atom; // [natoms] |d32 - d64| bound
-    const float*    S;
-    const uint16_t* P;
-    int             Lpad, Qp, i0, Q, T, K, box;
+    float*          S;
+    uint16_t*       P;
+    int             natoms, Lpad, Qp, i0, Q, T, K, box, rank_shift;
     long            pair_begin, pair_count;
-    const int2*     pair_ab; // optional [pair_count] (a1, a2) of an explicit pair list
+    const int2*     pair_ab;    // optional [pair_count] (a1, a2) of an explicit pair list
     const int*      pair_order; // optional task order: task k computes local pair pair_order[k]
-    int             staged;     // set by the launchers: coordinate rows staged in shared memory
-    int             shift;   // histogram bucket = 2^shift float ulps above the lower bound
-    uint32_t*       cnt;     // [T][pair_count] n_x | n_y << 16, or kHandOver
-    unsigned long long* wres;         // [Q][pair_count] walk results of the block
-    unsigned long long* hq;           // hand-over queue: cnt indices i * pair_count + pl
+    int             shift;      // histogram bucket = 2^shift float ulps above the lower bound
+    uint32_t*       cnt;        // [T][pair_count] n_x | n_y << 16, or kHandOver
+    unsigned long long* wres;   // [Q][pair_count] walk results of the block
+    unsigned long long* hq;     // hand-over queue: cnt indices i * pair_count + pl
     unsigned*           hq_len;
     unsigned            hq_cap;
-    unsigned long long* task_counter; // [2]: walk, finish
     int*                status;
     unsigned long long* walk_elems; // optional: total walked row entries
     unsigned*           reasons;    // optional [8]: hand-overs by cause
 };
 
-struct FixupParams
+// One launch over the query blocks of several trajectories (or of one): the
+// launch's tasks are numbered across the descriptors, descriptor d owning
+// tasks [prefix[d], prefix[d + 1]).  Every array lives in device memory.
+struct WalkBatch
 {
-    const double* X64;
-    int           T, K, box, rank_shift;
-    long          pair_begin, pair_count;
-    const int2*   pair_ab;
-    uint32_t*     cnt;
-    const unsigned long long* hq; // hand-over queue (may be null): entries are cnt indices
-    const unsigned*           hq_len;
-    unsigned                  hq_cap;
+    const WalkParams*   d;       // [n]
+    const long long*    rprefix; // [n + 1] row-sort tasks: natoms * Q per descriptor
+    const long long*    wprefix; // [n + 1] walk tasks: ceil(groups / walk warps) * pairs
+    const long long*    fprefix; // [n + 1] finish tasks: query groups * pairs
+    int                 n;
+    int                 maxT;    // largest frame count (shared-memory layout)
+    unsigned long long* counter; // [2] walk and finish task counters, zero at launch
 };
 
 // Bucket width of the walk histogram for k: about 1.3/k of the value
@@ -63,14 +63,20 @@ inline int walk_histogram_shift(int K)
     return s < 17 ? 17 : (s > 21 ? 21 : s);
 }
 
+// Walk launch shape for trajectories of up to maxT frames: warps per CTA and
+// whether the pair's coordinate rows are staged in shared memory.
+void walk_shape(int maxT, int* warps, bool* staged);
+// Largest walk warps per CTA that the staged layout allows (0: not staged).
+int walk_max_staged_warps(int maxT);
+
 // Each launcher returns the launch status (cudaGetLastError right after it).
 cudaError_t launch_ksg_x32(const double* X64, int natoms, int T, float4* X32, float* eps_atom, cudaStream_t s);
-cudaError_t launch_ksg_rows(const float4* X32, int natoms, int T, int i0, int Q, int Qp, int Lpad, float* S,
-                            uint16_t* P, cudaStream_t s);
-cudaError_t launch_ksg_walk(const WalkParams& p, int sms, cudaStream_t s);
-cudaError_t launch_ksg_finish(const WalkParams& p, int sms, cudaStream_t s);
-// Exact FP64 statistics for every queued hand-over, then for any hand-over
-// mark the queue could not hold (a scan of cnt).
-cudaError_t launch_ksg_fixup(const FixupParams& p, int sms, cudaStream_t s);
+cudaError_t launch_ksg_rows(const WalkBatch& b, long long rows, cudaStream_t s);
+cudaError_t launch_ksg_walk(const WalkBatch& b, int warps, bool staged, int sms, cudaStream_t s);
+cudaError_t launch_ksg_finish(const WalkBatch& b, int sms, cudaStream_t s);
+// Exact FP64 statistics for every queued hand-over of the batch's
+// descriptors, then for any hand-over mark a queue could not hold (a scan of
+// cnt).  One descriptor per trajectory.
+cudaError_t launch_ksg_fixup(const WalkBatch& b, int sms, cudaStream_t s);
 
 } // namespace gc

@@ -106,6 +106,19 @@ gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, do
  * not kept.  gc_release_cache frees every kept workspace. */
 void gc_release_cache(void);
 
+/* KSG MI matrices of ntraj trajectories in one batched run: trajectory i
+ * (its own atom and frame counts, nframes <= 16385) with k = ks[i] into
+ * mi[i] (natoms_i * natoms_i, the conventions of gc_ksg_matrix).  The query
+ * blocks of all trajectories share each launch of the row sort, walk and
+ * finish kernels (tasks drawn from every trajectory through one counter),
+ * the whole sequence runs as one captured CUDA graph, and the walk's launch
+ * shape is autotuned on the first call for a shape class.  The device
+ * workspace and graph of the last batch are kept for a repeated call with
+ * the same shapes; gc_ksg_batch_release frees them.  No counterpart in the
+ * reference, which handles one trajectory per run.  opts: device only. */
+gc_status gc_ksg_batch(const gc_traj_view* trajs, const int* ks, int ntraj, const gc_opts* opts, double* const* mi);
+void      gc_ksg_batch_release(void);
+
 /* Gaussian (linearized) MI matrix.  Replaces gauss_corrmatrix
  * (lib/correlation_core.h:76, lib/correlation_core.cpp:280-311). */
 gc_status gc_gauss_matrix(const gc_traj_view* traj, const gc_opts* opts, double* mi);

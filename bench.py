@@ -184,6 +184,39 @@ def run_reference(args):
     return 0
 
 
+def screened_variant(gc, x, k, plain_e2e_s: float, device: int, reps: int = 3):
+    """The MLP-screened matrix through gc_ksg_screened (host arrays in and
+    out, like the plain e2e leg): the calibrated rule of the committed model
+    (flag every pair whose ensemble spread exceeds the spread that kept the
+    audited error within 1e-2 on held-out trajectories), and the audit-only
+    rule (keep every prediction, exact KSG on the 5% audit sample only)."""
+    from gmx_correlation_b200.screen import TrainedScreen
+    ts = TrainedScreen.load(device=device)
+    n = x.shape[0]
+    pairs = n * (n - 1) // 2
+
+    def run(**kw):
+        gc.ksg_screened(x, k, ts.model, device=device, **kw)  # warm (plan shapes, pool)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            _, rep = gc.ksg_screened(x, k, ts.model, device=device, **kw)
+        dt = (time.perf_counter() - t0) / reps
+        return {"value": pairs / dt, "unit": UNIT, "speedup_vs_plain_e2e": plain_e2e_s / dt,
+                "exact_pairs": rep["exact"], "flagged": rep["flagged"], "audited": rep["audited"],
+                "audit_accepted": rep["audit_accepted"], "audited_max_dr": rep["audit_max_dr"],
+                "audited_rms_dr": rep["audit_rms_dr"], "final_max_dr": rep["final_max_dr"],
+                "ms_features": rep["ms_features"], "ms_mlp": rep["ms_mlp"], "ms_ksg": rep["ms_ksg"]}
+
+    cal = run()
+    cal["rule"] = {"sigma_max": ts.model.sigma_max, "margin": ts.model.margin, "audit_frac": 0.05,
+                   "target_max_dr": 1e-2}
+    loose = run(sigma_max=float("inf"), margin=0.0)
+    loose["rule"] = {"sigma_max": "inf", "margin": 0.0, "audit_frac": 0.05}
+    return {"model": {k2: ts.meta[k2] for k2 in ("trajectories", "train_pairs", "calib_rms", "gauss_rms",
+                                                 "calib_accept_frac") if k2 in ts.meta},
+            "calibrated_1e-2": cal, "audit_only": loose}
+
+
 def run_ours(args):
     import torch
 
@@ -296,6 +329,11 @@ def run_ours(args):
                                       f"FFMA {fma_flops / 1e12:.1f} TFLOP/s"},
             "clocks": clocks,
         }
+        if ws == 1 and not args.no_screen:
+            try:
+                out["screened"] = screened_variant(gc, x_pinned, k, e2e_s, local)
+            except Exception as e:  # noqa: BLE001
+                out["screened"] = {"unavailable": str(e)}
         if ws == 1 and not args.no_cpu_baseline:
             try:
                 out["cpu_baseline"] = cpu_baseline_sample(x, k, args.cpu_seconds)
@@ -317,6 +355,7 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-screen", action="store_true", help="skip the MLP-screened variant")
     ap.add_argument("--natoms", type=int, default=0, help="smaller atom count (profiling cases only)")
     ap.add_argument("--path", type=int, default=0, help="0 fast (default), 1 exact FP64")
     args = ap.parse_args(argv)

@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -33,6 +34,91 @@ using namespace gc::host;
 
 void gc::set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
 
+namespace {
+
+constexpr size_t kPoolCap = (size_t)48 << 30; // bytes a device's pool may hold
+
+struct DevicePool
+{
+    std::multimap<size_t, void*> blocks;
+    size_t                       bytes = 0;
+};
+// Never destroyed: blocks may still be returned while statics are torn down.
+std::mutex& g_pool_mutex = *new std::mutex;
+DevicePool* g_pool       = new DevicePool[64];
+
+int current_device()
+{
+    int d = -1;
+    if (cudaGetDevice(&d) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return -1;
+    }
+    return d < 64 ? d : -1;
+}
+
+} // namespace
+
+void* gc::host::pool_take(size_t bytes)
+{
+    const int d = current_device();
+    if (d < 0)
+        return nullptr;
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    auto                        it = g_pool[d].blocks.find(bytes);
+    if (it == g_pool[d].blocks.end())
+        return nullptr;
+    void* p = it->second;
+    g_pool[d].blocks.erase(it);
+    g_pool[d].bytes -= bytes;
+    return p;
+}
+
+void gc::host::pool_give(void* p, size_t bytes)
+{
+    cudaPointerAttributes attr{};
+    int                   d = -1;
+    if (cudaPointerGetAttributes(&attr, p) == cudaSuccess)
+        d = attr.device;
+    else
+        cudaGetLastError();
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mutex);
+        if (d >= 0 && d < 64 && g_pool[d].bytes + bytes <= kPoolCap)
+        {
+            g_pool[d].blocks.emplace(bytes, p);
+            g_pool[d].bytes += bytes;
+            return;
+        }
+    }
+    cudaFree(p);
+}
+
+void gc::host::pool_release()
+{
+    std::multimap<size_t, void*> all[64];
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mutex);
+        for (int d = 0; d < 64; ++d)
+        {
+            all[d].swap(g_pool[d].blocks);
+            g_pool[d].bytes = 0;
+        }
+    }
+    int prev = -1;
+    cudaGetDevice(&prev);
+    for (int d = 0; d < 64; ++d)
+        if (!all[d].empty())
+        {
+            cudaSetDevice(d);
+            for (auto& kv : all[d])
+                cudaFree(kv.second);
+        }
+    if (prev >= 0)
+        cudaSetDevice(prev);
+}
+
 // ---------------------------------------------------------------------------
 // KSG plan
 // ---------------------------------------------------------------------------
@@ -43,8 +129,8 @@ struct gc_ksg_plan
     int          natoms = 0, T = 0, K = 0, path = GC_PATH_AUTO;
     long         pair_begin = 0, pair_count = 0;
     cudaStream_t stream = nullptr;
-    DevBuf<double>   X, psi;
-    DevBuf<uint32_t> cnt;
+    PoolBuf<double>   X, psi;
+    PoolBuf<uint32_t> cnt;
     DevBuf<int>      status;
     DevBuf<int2>     pair_ab; // explicit pair list as (a1, a2), empty for a range
     int              launches = 0;
@@ -53,7 +139,7 @@ struct gc_ksg_plan
     bool                  fast = false;
     gc::host::KsgTraj     ft;
     gc::host::KsgLaunch   fl;
-    DevBuf<double>        io_xyz, io_mi; // gc_ksg_matrix staging of inputs and outputs
+    PoolBuf<double>       io_xyz, io_mi; // gc_ksg_matrix staging of inputs and outputs
     long                         reason_counts[8] = {};
     double                       walk_mean = 0.0;
     long                         handoffs = 0;
@@ -372,6 +458,7 @@ void gc_release_cache(void)
     for (gc_ksg_plan* p : plans)
         if (p)
             gc_ksg_plan_destroy(p);
+    gc::host::pool_release();
 }
 
 gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, double* mi)

@@ -104,6 +104,58 @@ struct DevBuf
     }
 };
 
+// Per-device pool of large device blocks (exact-size reuse): plans of the
+// same shape created one after another reuse the blocks instead of calling
+// cudaMalloc / cudaFree.  pool_release frees every pooled block.
+void* pool_take(size_t bytes);             // a block of exactly `bytes`, or nullptr
+void  pool_give(void* p, size_t bytes);    // keeps the block (or frees it when the pool is full)
+void  pool_release();
+
+// DevBuf whose blocks come from and return to the pool.
+template <class T>
+struct PoolBuf
+{
+    T*     p = nullptr;
+    size_t n = 0;
+    PoolBuf() = default;
+    PoolBuf(const PoolBuf&) = delete;
+    PoolBuf& operator=(const PoolBuf&) = delete;
+    ~PoolBuf() { reset(); }
+    void reset()
+    {
+        if (p)
+            pool_give(p, n * sizeof(T));
+        p = nullptr;
+        n = 0;
+    }
+    gc_status alloc(size_t count)
+    {
+        reset();
+        if (count == 0)
+            count = 1;
+        void* q = pool_take(count * sizeof(T));
+        if (!q)
+        {
+            cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+            if (e == cudaErrorMemoryAllocation)
+            {
+                cudaGetLastError();
+                pool_release(); // free what the pool holds and try once more
+                e = cudaMalloc(&q, count * sizeof(T));
+            }
+            if (e != cudaSuccess)
+            {
+                cudaGetLastError();
+                return fail(e == cudaErrorMemoryAllocation ? GC_ERR_OUT_OF_MEMORY : GC_ERR_CUDA,
+                            std::string("cudaMalloc: ") + cudaGetErrorString(e));
+            }
+        }
+        p = static_cast<T*>(q);
+        n = count;
+        return GC_OK;
+    }
+};
+
 inline gc_opts defaults()
 {
     gc_opts o;

@@ -63,8 +63,11 @@ struct BatchPlan
     }
 };
 
-std::mutex                 g_batch_mutex;
-std::unique_ptr<BatchPlan> g_batch[64];
+// Kept batches, one per device.  Deliberately never destroyed at process
+// exit (the driver frees device memory then), so no destructor runs after
+// the CUDA context is gone.
+std::mutex  g_batch_mutex;
+BatchPlan*  g_batch[64] = {};
 
 // Query-block size of every trajectory for the smallest number of waves
 // whose sorted rows fit the budget.
@@ -277,12 +280,15 @@ gc_status gc_ksg_batch(const gc_traj_view* trajs, const int* ks, int ntraj, cons
         key.insert(key.end(), {trajs[i].natoms, trajs[i].nframes, ks[i]});
 
     std::lock_guard<std::mutex> lock(g_batch_mutex); // one batch per process at a time
-    std::unique_ptr<BatchPlan>& bp = g_batch[cur];
-    if (!bp || bp->key != key)
+    if (!g_batch[cur] || g_batch[cur]->key != key)
     {
-        bp.reset();
-        GC_TRY(create_plan(trajs, ks, ntraj, cur, bp));
+        delete g_batch[cur];
+        g_batch[cur] = nullptr;
+        std::unique_ptr<BatchPlan> made;
+        GC_TRY(create_plan(trajs, ks, ntraj, cur, made));
+        g_batch[cur] = made.release();
     }
+    BatchPlan* bp = g_batch[cur];
     cudaStream_t s = bp->stream;
     for (int i = 0; i < ntraj; ++i)
         GC_TRY(upload_traj(&trajs[i], bp->t[(size_t)i]->xyz.p, s));
@@ -326,11 +332,12 @@ gc_status gc_ksg_batch(const gc_traj_view* trajs, const int* ks, int ntraj, cons
 void gc_ksg_batch_release(void)
 {
     std::lock_guard<std::mutex> lock(g_batch_mutex);
-    for (auto& b : g_batch)
+    for (BatchPlan*& b : g_batch)
         if (b)
         {
             DeviceScope dev(b->device);
-            b.reset();
+            delete b;
+            b = nullptr;
         }
 }
 

@@ -32,12 +32,12 @@ struct KsgTraj
     unsigned hq_cap = 0;
     const int2* d_pair_ab = nullptr; // explicit list as (a1, a2) (owned by the caller), or null
     std::vector<long> list;          // host copy of the list's pair indices (for the tile order)
-    DevBuf<float4>             X32;
-    DevBuf<float>              eps, S;
-    DevBuf<uint16_t>           P;
-    DevBuf<unsigned long long> wres, hq, walk_elems;
-    DevBuf<unsigned>           hq_len, reasons;
-    DevBuf<int>                pair_order;
+    PoolBuf<float4>             X32;
+    PoolBuf<float>              eps, S;
+    PoolBuf<uint16_t>           P;
+    PoolBuf<unsigned long long> wres, hq, walk_elems;
+    PoolBuf<unsigned>           hq_len, reasons;
+    PoolBuf<int>                pair_order;
 
     // Sizes the workspace for query blocks of Q frames (a multiple of 32, or T).
     gc_status create(int natoms, int T, int K, long pair_begin, long pair_count, const int64_t* list,

@@ -482,12 +482,13 @@ __device__ __forceinline__ void task_pair(const WalkParams& p, long k, Task& tk)
 }
 
 __device__ __forceinline__ bool next_task(const WalkBatch& B, long long total, long long* s_task, int* s_desc,
-                                          Task& tk, int& d)
+                                          int* s_next, Task& tk, int& d)
 {
     if (threadIdx.x == 0)
     {
         const long long t = (long long)atomicAdd(B.counter, 1ull);
         *s_task           = t;
+        *s_next           = 0;
         if (t < total)
             *s_desc = batch_desc(B.wprefix, B.n, t);
     }
@@ -520,8 +521,8 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ long long s_task;
-    __shared__ int       s_desc;
-    const int            warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    __shared__ int       s_desc, s_next;
+    const int            warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float4*              sx   = reinterpret_cast<float4*>(smem_raw);
     unsigned char*       base = smem_raw + (STAGED ? (size_t)2 * B.maxT * 16 : 0) + (size_t)warp * kWalkBuckets * 32;
     // bucket b of this lane: byte b % 4 of word (b / 4) * 32 + lane, so the
@@ -533,7 +534,7 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
     const float     inf   = __int_as_float(0x7f800000);
     Task            tk;
     int             dsc;
-    while (next_task(B, total, &s_task, &s_desc, tk, dsc))
+    while (next_task(B, total, &s_task, &s_desc, &s_next, tk, dsc))
     {
         const WalkParams& p       = B.d[dsc];
         const int         T       = p.T, K = p.K, Llen = T - 1, shift = p.shift;
@@ -551,7 +552,17 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
             xa = sx;
             xb = sx + T;
         }
-        const int       g    = tk.c * warps + warp;
+        // the task's query groups go to whichever warp asks next, so warps
+        // that finish early take more groups of the same pair
+        for (;;)
+        {
+        int gi = 0;
+        if (lane == 0)
+            gi = atomicAdd(&s_next, 1);
+        gi = __shfl_sync(kFull, gi, 0);
+        const int g = tk.c * B.chunk + gi;
+        if (gi >= B.chunk || g >= ngroups)
+            break;
         const int       iq   = g * 32 + lane;
         const bool      live = g < ngroups && iq < p.Q;
         const int       iql  = live ? iq : 0;
@@ -668,7 +679,9 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
             if (lane == 0 && we)
                 atomicAdd(p.walk_elems, (unsigned long long)we);
         }
-        __syncthreads(); // every warp is done with the staged rows and its histogram
+        __syncwarp(); // the next group clears this warp's histogram
+        }
+        __syncthreads(); // every warp is done with the staged rows
     }
 }
 

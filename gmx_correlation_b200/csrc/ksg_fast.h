@@ -46,10 +46,11 @@ struct WalkBatch
 {
     const WalkParams*   d;       // [n]
     const long long*    rprefix; // [n + 1] row-sort tasks: natoms * Q per descriptor
-    const long long*    wprefix; // [n + 1] walk tasks: ceil(groups / walk warps) * pairs
+    const long long*    wprefix; // [n + 1] walk tasks: ceil(groups / chunk) * pairs
     const long long*    fprefix; // [n + 1] finish tasks: query groups * pairs
     int                 n;
     int                 maxT;    // largest frame count (shared-memory layout)
+    int                 chunk;   // query groups per walk task (shared by the CTA's warps)
     unsigned long long* counter; // [2] walk and finish task counters, zero at launch
 };
 

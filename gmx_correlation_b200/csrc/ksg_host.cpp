@@ -148,7 +148,8 @@ gc_status KsgLaunch::build(const std::vector<std::vector<WalkParams>>& wave_desc
             maxT                 = std::max(maxT, d.T);
             const long long grp  = (d.Q + 31) / 32;
             r += (long long)d.natoms * d.Q;
-            w += (grp + cfg.walk_warps - 1) / cfg.walk_warps * d.pair_count;
+            const long long chunk = (long long)cfg.walk_warps * cfg.chunk_mult;
+            w += (grp + chunk - 1) / chunk * d.pair_count;
             f += grp * d.pair_count;
             rp.push_back(r);
             wp.push_back(w);
@@ -177,6 +178,7 @@ gc_status KsgLaunch::build(const std::vector<std::vector<WalkParams>>& wave_desc
         b.fprefix  = b.wprefix + (n + 1);
         b.n        = n;
         b.maxT     = maxT;
+        b.chunk    = cfg.walk_warps * cfg.chunk_mult;
         b.counter  = counters.p + 2 * v;
         waves.push_back(b);
         wave_rows.push_back(pre[pofs[v] + n]);
@@ -246,25 +248,28 @@ std::vector<WalkConfig> walk_candidates(int maxT)
             if (w <= wmax && std::find(warps.begin(), warps.end(), w) == warps.end())
                 warps.push_back(w);
     }
-    for (int tile : {8, 16, 32})
-    {
-        if (warps.empty())
+    for (int tile : {16, 32})
+        for (int mult : {1, 2, 4})
         {
-            WalkConfig c;
-            c.walk_warps = kWalkWarps;
-            c.staged     = false;
-            c.pair_tile  = tile;
-            out.push_back(c);
+            if (warps.empty())
+            {
+                WalkConfig c;
+                c.walk_warps = kWalkWarps;
+                c.staged     = false;
+                c.pair_tile  = tile;
+                c.chunk_mult = mult;
+                out.push_back(c);
+            }
+            for (int w : warps)
+            {
+                WalkConfig c;
+                c.walk_warps = w;
+                c.staged     = true;
+                c.pair_tile  = tile;
+                c.chunk_mult = mult;
+                out.push_back(c);
+            }
         }
-        for (int w : warps)
-        {
-            WalkConfig c;
-            c.walk_warps = w;
-            c.staged     = true;
-            c.pair_tile  = tile;
-            out.push_back(c);
-        }
-    }
     return out;
 }
 

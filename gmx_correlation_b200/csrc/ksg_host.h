@@ -18,6 +18,7 @@ struct WalkConfig
     int  walk_warps = 0;
     bool staged     = false;
     int  pair_tile  = 16;
+    int  chunk_mult = 4; // query groups per walk task = chunk_mult * walk_warps
 };
 
 // Fast-path workspace of one trajectory (all pairs, a shard, or a list): the

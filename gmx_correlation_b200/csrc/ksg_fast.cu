@@ -325,6 +325,15 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
         S[idx]                       = __uint_as_float((unsigned)(k >> 32));
         P[idx]                       = (uint16_t)(k & 0xFFFFu);
     }
+    // the last 4-entry group runs out in NaN (never <= any stop value) with
+    // frame 0, so the walk reads whole groups without a bounds test
+    if (tid < ((N + 3) & ~3) - N)
+    {
+        const int    m   = N + tid;
+        const size_t idx = base + (size_t)(m >> 2) * gstride + (m & 3);
+        S[idx]           = __int_as_float(0x7fc00000);
+        P[idx]           = 0;
+    }
 }
 
 namespace {
@@ -515,8 +524,11 @@ __device__ __forceinline__ unsigned long long pack_walk(int bstar, int prefix, i
 } // namespace
 
 // Pass 1: walk the sorted row, histogram v = max(s, d) per lane.  STAGED:
-// the pair's coordinate rows are copied into shared memory per task.
-template <bool STAGED>
+// the pair's coordinate rows are copied into shared memory per task.  LO
+// (every k of the launch below 256): entries below the lower bound L count
+// in histogram index 0 (at most k - 1 of them: they all have s < L, the k-th
+// walked-row value), so the per-entry update needs no separate test.
+template <bool STAGED, bool LO>
 __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -525,10 +537,11 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
     const int            warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float4*              sx   = reinterpret_cast<float4*>(smem_raw);
     unsigned char*       base = smem_raw + (STAGED ? (size_t)2 * B.maxT * 16 : 0) + (size_t)warp * kWalkBuckets * 32;
-    // bucket b of this lane: byte b % 4 of word (b / 4) * 32 + lane, so the
-    // 32 lanes of a warp always hit 32 different banks
+    // histogram index b of this lane: byte b % 4 of word (b / 4) * 32 + lane,
+    // so the 32 lanes of a warp always hit 32 different banks
     uint8_t* hist = base + lane * 4;
     auto     H    = [hist](unsigned b) -> uint8_t& { return hist[(b >> 2) * 128 + (b & 3)]; };
+    constexpr unsigned kTop = kWalkBuckets - 1; // open-ended index above the range, never read
 
     const long long total = B.wprefix[B.n];
     const float     inf   = __int_as_float(0x7f800000);
@@ -576,18 +589,30 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
         }
         __syncwarp();
 
-        // Buckets are 2^shift float ulps above L; v < L counts in cnt_lo.  Every
-        // 16 entries the buckets below the current value are final (later
-        // entries have v >= s), so their running sum R decides the stop value.
+        // Histogram index of v: LO: 0 for v < L, then buckets of 2^shift
+        // float ulps from L; otherwise buckets from L (v < L counted in
+        // cnt_lo).  Index b starts at value bits Lh + (b << shift) (b >= 1
+        // when LO); the last index takes everything above the range.
+        const unsigned Lh   = LO ? u.Lb - (1u << shift) : u.Lb;
+        auto           hidx = [Lh, shift](float v) -> unsigned {
+            if (LO)
+                return (unsigned)min(max((int)(__float_as_uint(v) - Lh) >> shift, 0), (int)kTop);
+            return min((__float_as_uint(v) - Lh) >> shift, kTop);
+        };
+        // Every 16 entries the indices below the current value are final
+        // (later entries have v >= s), so their running sum R decides the stop
+        // value.  The rows end in NaN up to a 4-entry boundary, which the
+        // take test (s <= stop) never passes, so taken entries form a prefix
+        // of each group and a group short of 4 ends the walk.
         const float4* Sg = reinterpret_cast<const float4*>(u.rw.S); // 4-entry groups of this lane's row
         const uint2*  Pg = reinterpret_cast<const uint2*>(u.rw.P);
         const size_t  gs = (size_t)p.Qp;                            // group stride
-        int           m = 0, cnt_lo = 0, R = 0, thr = 0, grp = 0;
-        float         stop      = inf;
-        bool          saturated = false; // a bucket below the last one passed 255
-        bool          walking   = live;
-        float4        s4        = make_float4(inf, inf, inf, inf);
-        uint2         j4        = make_uint2(0u, 0u);
+        int           m_end = 0, cnt_lo = 0, R = 0, thr = 0, grp = 0;
+        unsigned      wrap = 0u; // bit 8 set once a counter below the top passed 255
+        float         stop = inf;
+        bool          walking = live;
+        float4        s4      = make_float4(inf, inf, inf, inf);
+        uint2         j4      = make_uint2(0u, 0u);
         if (live)
         {
             s4 = Sg[0];
@@ -597,59 +622,66 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
         while (walking)
         {
             if (grp > last) // the whole row walked
+            {
+                m_end = Llen;
                 break;
+            }
             // prefetch the next group (the last group again at the end)
-            const int    nxt   = grp < last ? grp + 1 : grp;
-            const float4 ns4   = Sg[(size_t)nxt * gs];
-            const uint2  nj4   = Pg[(size_t)nxt * gs];
-            const int    valid = Llen - grp * 4; // entries of this group inside the row (>= 1)
-            const float  sv[4] = {s4.x, s4.y, s4.z, s4.w};
+            const int      nxt   = grp < last ? grp + 1 : grp;
+            const float4   ns4   = Sg[(size_t)nxt * gs];
+            const uint2    nj4   = Pg[(size_t)nxt * gs];
+            const float    sv[4] = {s4.x, s4.y, s4.z, s4.w};
             const unsigned jv[4] = {j4.x & 0xFFFFu, j4.x >> 16, j4.y & 0xFFFFu, j4.y >> 16};
-            int            ntk   = 0;
-            // Branch-free: every slot gathers (frame 0 when not taken) and
-            // updates its bucket by 0 or 1; taken entries form a prefix.
+            bool           tkn[4];
+            // Branch-free: every slot gathers and adds 0 or 1 to its counter.
 #pragma unroll
             for (int q = 0; q < 4; ++q)
             {
-                const bool     take  = q < valid && sv[q] <= stop;
-                const float    v     = fmaxf(sv[q], dist3f(u.xo, X32o[take ? jv[q] : 0u]));
-                const bool     below = v < u.L;
-                const bool     inc   = take && !below;
-                const unsigned b     = min((__float_as_uint(v) - u.Lb) >> shift, (unsigned)kWalkBuckets - 1);
-                uint8_t&       c     = H(b);
-                const unsigned h     = c;
-                c                    = (uint8_t)(h + (inc ? 1u : 0u));
-                saturated |= inc && h == 255u && b < kWalkBuckets - 1;
-                ntk += take;
-                cnt_lo += take && below;
+                tkn[q]          = sv[q] <= stop;
+                const float v   = fmaxf(sv[q], dist3f(u.xo, X32o[jv[q]]));
+                bool        inc = tkn[q];
+                if (!LO)
+                {
+                    const bool below = v < u.L;
+                    cnt_lo += inc && below;
+                    inc = inc && !below;
+                }
+                uint8_t&       c  = H(hidx(v));
+                const unsigned h1 = (unsigned)c + (inc ? 1u : 0u);
+                c                 = (uint8_t)h1;
+                wrap |= h1;
             }
-            m += ntk;
             ++grp;
-            if (ntk < 4)
-                walking = false;
-            else if (stop == inf && (grp & 3) == 0)
+            if (!tkn[3])
             {
-                const float sl = sv[3];
-                const int   bn =
-                    sl >= u.L ? (int)min((__float_as_uint(sl) - u.Lb) >> shift, (unsigned)kWalkBuckets - 1) : 0;
-                for (int b = thr; b < bn; ++b)
-                    R += H(b);
-                thr = max(thr, bn);
-                if (cnt_lo + R >= K)
-                    stop = __fadd_ru(__uint_as_float(u.Lb + ((unsigned)bn << shift)), u.e2);
+                walking = false;
+                m_end   = (grp - 1) * 4 + (int)tkn[0] + (int)tkn[1] + (int)tkn[2];
+            }
+            else if ((grp & 3) == 0)
+            {
+                H(kTop) = 0; // at most 16 increments between clears: never wraps
+                if (stop == inf)
+                {
+                    const float sl = sv[3];
+                    const int   bn = (LO || sl >= u.L) ? (int)hidx(sl) : 0;
+                    for (int b = thr; b < bn; ++b)
+                        R += H(b);
+                    thr = max(thr, bn);
+                    if (cnt_lo + R >= K)
+                        stop = __fadd_ru(__uint_as_float(Lh + ((unsigned)bn << shift)), u.e2);
+                }
             }
             s4 = ns4;
             j4 = nj4;
         }
-        const int m_end = m;
 
-        // bucket of the k-th value
+        // histogram index of the k-th value
         if (live)
         {
             int bstar, prefix;
             if (stop != inf)
             {
-                // cum = #{v < edge(b + 1)} >= K; step down while still >= K
+                // cum = #{v below index b + 1} >= K; step down while still >= K
                 int cum = cnt_lo + R, b = thr - 1;
                 while (b > 0 && cum - (int)H(b) >= K)
                 {
@@ -662,7 +694,7 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
             else
             {
                 int cum = cnt_lo, b = 0;
-                while (b < kWalkBuckets - 1 && cum + (int)H(b) < K)
+                while (b < (int)kTop && cum + (int)H(b) < K)
                 {
                     cum += H(b);
                     ++b;
@@ -670,8 +702,12 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
                 bstar  = b;
                 prefix = cum;
             }
-            const int reason = saturated ? kReasonBand : (bstar >= kWalkBuckets - 1 ? kReasonRange : 0);
-            p.wres[(size_t)iq * p.pair_count + tk.pl] = pack_walk(bstar, prefix, m_end, reason);
+            // index 0 under LO holds fewer than k entries, so the k-th value
+            // lies above it unless the input is not finite
+            const int reason = (wrap > 255u || (LO && bstar == 0)) ? kReasonBand
+                               : (bstar >= (int)kTop ? kReasonRange : 0);
+            // the result names buckets from L (index - 1 under LO)
+            p.wres[(size_t)iq * p.pair_count + tk.pl] = pack_walk(LO ? bstar - 1 : bstar, prefix, m_end, reason);
         }
         if (p.walk_elems)
         {
@@ -1182,7 +1218,9 @@ void walk_shape(int maxT, int* warps, bool* staged)
 
 cudaError_t launch_ksg_walk(const WalkBatch& b, int warps, bool staged, int sms, cudaStream_t s)
 {
-    void (*kernel)(WalkBatch) = staged ? ksg_walk_kernel<true> : ksg_walk_kernel<false>;
+    const bool lo = b.maxK < 256;
+    void (*kernel)(WalkBatch) = staged ? (lo ? ksg_walk_kernel<true, true> : ksg_walk_kernel<true, false>)
+                                       : (lo ? ksg_walk_kernel<false, true> : ksg_walk_kernel<false, false>);
     const size_t smem = (staged ? (size_t)2 * b.maxT * 16 : 0) + (size_t)warps * kWalkBuckets * 32;
     cudaError_t  e    = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)

@@ -50,6 +50,7 @@ struct WalkBatch
     const long long*    fprefix; // [n + 1] finish tasks: query groups * pairs
     int                 n;
     int                 maxT;    // largest frame count (shared-memory layout)
+    int                 maxK;    // largest k
     int                 chunk;   // query groups per walk task (shared by the CTA's warps)
     unsigned long long* counter; // [2] walk and finish task counters, zero at launch
 };

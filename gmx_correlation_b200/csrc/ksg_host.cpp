@@ -135,7 +135,7 @@ gc_status KsgLaunch::build(const std::vector<std::vector<WalkParams>>& wave_desc
     std::vector<WalkParams> all;
     std::vector<long long>  pre;
     std::vector<size_t>     dofs, pofs;
-    int                     maxT = 0;
+    int                     maxT = 0, maxK = 0;
     for (const auto& wv : wave_descs)
     {
         dofs.push_back(all.size());
@@ -146,6 +146,7 @@ gc_status KsgLaunch::build(const std::vector<std::vector<WalkParams>>& wave_desc
         {
             all.push_back(d);
             maxT                 = std::max(maxT, d.T);
+            maxK                 = std::max(maxK, d.K);
             const long long grp  = (d.Q + 31) / 32;
             r += (long long)d.natoms * d.Q;
             const long long chunk = (long long)cfg.walk_warps * cfg.chunk_mult;
@@ -178,6 +179,7 @@ gc_status KsgLaunch::build(const std::vector<std::vector<WalkParams>>& wave_desc
         b.fprefix  = b.wprefix + (n + 1);
         b.n        = n;
         b.maxT     = maxT;
+        b.maxK     = maxK;
         b.chunk    = cfg.walk_warps * cfg.chunk_mult;
         b.counter  = counters.p + 2 * v;
         waves.push_back(b);
@@ -187,6 +189,7 @@ gc_status KsgLaunch::build(const std::vector<std::vector<WalkParams>>& wave_desc
     fix.d    = descs.p + tofs;
     fix.n    = (int)traj_descs.size();
     fix.maxT = maxT;
+    fix.maxK = maxK;
     return GC_OK;
 }
 

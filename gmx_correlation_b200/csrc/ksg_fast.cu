@@ -728,18 +728,19 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
     const int      warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* base = smem_raw + (size_t)warp * kBandSlotBytes * kBandCap * 32;
     // per-lane columns: band entry e of lane l at [e * 32 + l]: joint value v,
-    // walked-marginal value s, other-marginal value d, row position (>= 0 in
-    // the walked row, -1 - position in the other row) and frame
+    // walked-marginal value s, other-marginal value d and the row position as
+    // an offset from the start of its range (the walked-row range holds the
+    // first entries, the other-row range the rest)
     float*    bv = reinterpret_cast<float*>(base) + lane;
     float*    bs = bv + kBandCap * 32;
     float*    bd = bs + kBandCap * 32;
-    int*      bp = reinterpret_cast<int*>(bd + kBandCap * 32);
-    uint16_t* bj = reinterpret_cast<uint16_t*>(reinterpret_cast<float*>(base) + 4 * kBandCap * 32) + lane;
+    uint16_t* bo = reinterpret_cast<uint16_t*>(bd + kBandCap * 32 - lane) + lane;
 
     const long long total = B.fprefix[B.n];
     for (;;)
     {
-        // warp task: query group g outer, pairs (in tile order) inner
+        // warp task: query group g outer, pairs (in tile order) inner, so
+        // the warps running at once share the sorted rows of a query group
         long long t   = 0;
         int       dsc = 0;
         if (lane == 0)
@@ -797,14 +798,13 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
                 row_bounds4(rr, lo, hi, tt, st);
                 const int mw0 = lo[0], mw1 = lo[1], mo0 = lo[2], mo1 = lo[3];
                 int       nband = 0, nlo = 0;
-                auto add = [&](float v, float sv, float dv, int j, int pos) {
+                auto add = [&](float v, float sv, float dv, int off) {
                     if (nband < kBandCap)
                     {
                         bv[nband * 32] = v;
                         bs[nband * 32] = sv;
                         bd[nband * 32] = dv;
-                        bp[nband * 32] = pos;
-                        bj[nband * 32] = (uint16_t)j;
+                        bo[nband * 32] = (uint16_t)off;
                     }
                     ++nband;
                     nlo += v < elo;
@@ -834,9 +834,10 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
                             const float sv = f4get(s4[h], q);
                             const float dv = dist3f(xo, X32o[in ? j : 0]);
                             if (in && dv <= bandhi)
-                                add(fmaxf(sv, dv), sv, dv, j, mm);
+                                add(fmaxf(sv, dv), sv, dv, mm - mw0);
                         }
                 }
+                const int nW = nband; // band entries from the walked row come first
                 for (int g0 = mo0 >> 2; g0 * 4 < mo1; g0 += 2) // d in the band, s < inlo
                 {
                     float4 d4[2];
@@ -859,9 +860,13 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
                             const float dv = f4get(d4[h], q);
                             const float sv = dist3f(xw, X32w[in ? j : 0]);
                             if (in && sv < inlo)
-                                add(dv, sv, dv, j, -1 - mm);
+                                add(dv, sv, dv, mm - mo0);
                         }
                 }
+                // frame of band entry e (for the FP64 paths)
+                auto band_frame = [&](int e) -> int {
+                    return e < nW ? rw.j(mw0 + bo[e * 32]) : ro.j(mo0 + bo[e * 32]);
+                };
                 int       n_in = prefix - nlo; // #{v < inlo}
                 const int r    = K - n_in;     // 1-based rank of the k-th value in the band
                 if (!reason && (nband > kBandCap || r < 1 || r > nband))
@@ -932,7 +937,7 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
                         for (unsigned am = amb; am; am &= am - 1, ++c)
                         {
                             const int    e  = __ffs(am) - 1;
-                            const int    j  = bj[e * 32];
+                            const int    j  = band_frame(e);
                             const double dw = dist3r(xw64, T, qw0, qw1, qw2, j);
                             const double dq = dist3r(xo64, T, qo0, qo1, qo2, j);
                             slot[c]         = e;
@@ -967,8 +972,8 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
                         if (!(bv[e * 32] < lower || ((amem >> e) & 1u)))
                             continue;
                         const float val  = bval[e * 32];
-                        const int   pos  = bp[e * 32];
-                        const int   prow = side == 0 ? (pos >= 0 ? pos : -1) : (pos < 0 ? -1 - pos : -1);
+                        // row position of the entry in this side's row (-1: other row)
+                        const int   prow = (side == 0) == (e < nW) ? (side == 0 ? mw0 : mo0) + bo[e * 32] : -1;
                         if (val > top)
                         {
                             sec  = top;
@@ -1058,7 +1063,7 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
                     double       best = -1.0;
                     for (int e = 0; e < nband; ++e)
                         if ((bv[e * 32] < lower || ((amem >> e) & 1u)) && bval[e * 32] >= tie)
-                            best = fmax(best, dist3r(x64, T, q0, q1, q2, bj[e * 32]));
+                            best = fmax(best, dist3r(x64, T, q0, q1, q2, band_frame(e)));
                     for (int pos = first; pos >= 0; --pos)
                     {
                         const float sv = row.s(pos);

@@ -10,7 +10,7 @@ constexpr int kWalkWarps   = 32;       // most warps per walk CTA
 constexpr int kFinishWarps = 16;       // warps per finish CTA
 constexpr int kWalkBuckets = 128;      // per-lane histogram buckets
 constexpr int kBandCap     = 20;       // band entries kept per lane
-constexpr int kBandSlotBytes = 18;     // v, s, d (f32), row position (i32), frame (u16)
+constexpr int kBandSlotBytes = 14;     // v, s, d (f32), row position in its range (u16)
 constexpr uint32_t kHandOver = 0xFFFFFFFFu; // cnt value of a query handed to the exact kernel
 
 // Sorted marginal rows of one query block, transposed so that the 32

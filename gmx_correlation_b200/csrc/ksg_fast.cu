@@ -103,13 +103,20 @@ __device__ __forceinline__ int batch_desc(const long long* __restrict__ prefix, 
 // excluded), sorted ascending with their frames.  Keys are
 // (distance bits << 32 | frame).  A bucket pass over the row's own
 // distribution (range, coarse CDF, histogram, scan, scatter) leaves about one
-// key per bucket, which one thread per bucket insertion-sorts.  Distances are
-// recomputed from the atom's coordinate row (L1-resident) in every pass
-// rather than kept in shared memory.  A row with a crowded bucket (more than
-// 64 equal-ish distances, e.g. duplicated frames), and rows longer than 8192,
+// key per bucket, which one thread per bucket insertion-sorts.  R > 0: each
+// thread keeps its R distances (entries tid + r * threads) in registers for
+// the passes; R = 0: distances are recomputed from the atom's coordinate row
+// (L1-resident) in every pass.  A row with a crowded bucket (more than 64
+// equal-ish distances, e.g. duplicated frames), and rows longer than 8192,
 // are sorted by a bitonic network instead.
 constexpr int kRowsThreads = 256;
 
+// Bucket counters and cursors carry one padding word per 32, so the
+// contiguous bucket slices a thread scans start in distinct banks.
+__device__ __forceinline__ int rows_skew(int b) { return b + (b >> 5); }
+__host__ __device__ constexpr int rows_skewed(int nbin) { return nbin + (nbin >> 5); }
+
+template <int R>
 __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
 {
     extern __shared__ __align__(16) unsigned char rows_smem[];
@@ -135,8 +142,8 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
     // bucket pass up to 8192 keys; longer rows use the bitonic network alone
     const int           nbin   = N2 <= 8192 ? (N2 < 4096 ? N2 : 4096) : 0;
     unsigned long long* keys   = reinterpret_cast<unsigned long long*>(rows_smem); // [N2] sorted output
-    unsigned*           hist   = reinterpret_cast<unsigned*>(keys + N2);           // [nbin]
-    unsigned*           cursor = hist + nbin;                                      // [nbin]
+    unsigned*           hist   = reinterpret_cast<unsigned*>(keys + N2);           // [skewed nbin]
+    unsigned*           cursor = hist + rows_skewed(nbin);                         // [skewed nbin]
     float*              S      = w.S;
     uint16_t*           P      = w.P;
     const float4*       X32    = w.X32;
@@ -144,14 +151,42 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
     const float4  q   = xr[i];
     auto          frame_of = [i](int m) { return m < i ? m : m + 1; };
 
-    unsigned kmin = 0xFFFFFFFFu, kmax = 0u;
-    for (int m = tid; m < N; m += kRowsThreads)
+    // the row's distances, entry m = tid + k * threads
+    float dreg[R > 0 ? R : 1];
+    if constexpr (R > 0)
     {
-        const unsigned k = __float_as_uint(dist3f(q, xr[frame_of(m)]));
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const int m = tid + k * kRowsThreads;
+            dreg[k]     = m < N ? dist3f(q, xr[frame_of(m)]) : 0.0f;
+        }
+    }
+    auto each = [&](auto&& fn) {
+        if constexpr (R > 0)
+        {
+#pragma unroll
+            for (int k = 0; k < R; ++k)
+            {
+                const int m = tid + k * kRowsThreads;
+                if (m < N)
+                    fn(m, dreg[k]);
+            }
+        }
+        else
+        {
+            for (int m = tid; m < N; m += kRowsThreads)
+                fn(m, dist3f(q, xr[frame_of(m)]));
+        }
+    };
+
+    unsigned kmin = 0xFFFFFFFFu, kmax = 0u;
+    each([&](int, float d) {
+        const unsigned k = __float_as_uint(d);
         kmin             = min(kmin, k);
         kmax             = max(kmax, k);
-    }
-    for (int b = tid; b < nbin; b += kRowsThreads)
+    });
+    for (int b = tid; b < rows_skewed(nbin); b += kRowsThreads)
         hist[b] = 0u;
     for (int e = lane; e < 64; e += 32)
         coarse[warp][e] = 0u;
@@ -190,11 +225,11 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
         frac             = fminf(t - (float)c, 1.0f);
         return c;
     };
-    for (int m = tid; m < N && nbin; m += kRowsThreads)
-    {
-        float f;
-        atomicAdd(&coarse[warp][coarse_of(dist3f(q, xr[frame_of(m)]), f)], 1u);
-    }
+    if (nbin)
+        each([&](int, float d) {
+            float f;
+            atomicAdd(&coarse[warp][coarse_of(d, f)], 1u);
+        });
     __syncthreads();
     if (warp == 0)
     {
@@ -221,21 +256,21 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
     }
     __syncthreads();
     const float fscale = (float)nbin / fmaxf((float)N, 1.0f);
-    auto bin_of = [&](float v) -> unsigned {
+    auto bin_of = [&](float v) -> int {
         float          f;
         const unsigned c = coarse_of(v, f);
         const unsigned b = (unsigned)((cum[c] + f * (cum[c + 1] - cum[c])) * fscale);
-        return b < (unsigned)nbin ? b : (unsigned)nbin - 1;
+        return rows_skew(b < (unsigned)nbin ? (int)b : nbin - 1);
     };
     // histogram
-    for (int m = tid; m < N && nbin; m += kRowsThreads)
-        atomicAdd(&hist[bin_of(dist3f(q, xr[frame_of(m)]))], 1u);
+    if (nbin)
+        each([&](int, float d) { atomicAdd(&hist[bin_of(d)], 1u); });
     __syncthreads();
     // exclusive scan of hist into cursor (each thread a contiguous slice)
     const int per = nbin / kRowsThreads; // 0 without a bucket pass
     unsigned  loc = 0;
     for (int e = 0; e < per; ++e)
-        loc += hist[tid * per + e];
+        loc += hist[rows_skew(tid * per + e)];
     unsigned incl = loc;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1)
@@ -253,8 +288,9 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
     unsigned run = wbase + incl - loc;
     for (int e = 0; e < per; ++e)
     {
-        const unsigned c      = hist[tid * per + e];
-        cursor[tid * per + e] = run;
+        const int      b = rows_skew(tid * per + e);
+        const unsigned c = hist[b];
+        cursor[b]        = run;
         if (c > 64)
             crowded = 1;
         run += c;
@@ -262,22 +298,22 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
     __syncthreads();
     // scatter (or place in frame order for the bitonic network)
     const bool bucketed = !crowded;
-    for (int m = tid; m < N; m += kRowsThreads)
-    {
+    each([&](int m, float d) {
         const int                j   = frame_of(m);
-        const float              d   = dist3f(q, xr[j]);
         const unsigned long long k   = ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)j;
         const unsigned           pos = bucketed ? atomicAdd(&cursor[bin_of(d)], 1u) : (unsigned)m;
         keys[pos]                    = k;
-    }
+    });
     __syncthreads();
     if (bucketed)
     {
-        // cursor[b] now holds the end of bucket b; sort each bucket
-        for (int e = 0; e < per; ++e)
+        // cursor[b] now holds the end of bucket b; sort each bucket (thread
+        // t takes buckets t, t + threads, ..., so a warp's buckets, and
+        // their keys, lie side by side)
+        for (int b = tid; b < nbin; b += kRowsThreads)
         {
-            const int      b   = tid * per + e;
-            const unsigned end = cursor[b], beg = end - hist[b];
+            const int      bs  = rows_skew(b);
+            const unsigned end = cursor[bs], beg = end - hist[bs];
             for (unsigned x = beg + 1; x < end; ++x)
             {
                 const unsigned long long v = keys[x];
@@ -984,10 +1020,14 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
                             sec = val;
                     }
                     // members with v < inlo: the first one below the band start
-                    // in this row holds their maximum (a 4-entry group per round)
-                    int   mm = (side == 0 ? mw0 : mo0) - 1, first = -1;
-                    float fval = -1.0f, fsec = -1.0f;
-                    while (mm >= 0 && first < 0)
+                    // in this row holds their maximum (a 4-entry group per round).
+                    // Row values below the band start are < inlo, so when a band
+                    // member already tops inlo by 2 eps they can neither be the
+                    // maximum nor lie within 2 eps of it: no scan.
+                    const bool settled = top >= 0.0f && __fsub_rd(top, __fmul_ru(2.0f, eps)) >= inlo;
+                    int        mm = (side == 0 ? mw0 : mo0) - 1, first = -1;
+                    float      fval = -1.0f, fsec = -1.0f;
+                    while (!settled && mm >= 0 && first < 0)
                     {
                         const int    g  = mm >> 2;
                         const float4 s4 = row.s4(g);
@@ -1190,13 +1230,19 @@ cudaError_t launch_ksg_rows(const WalkBatch& b, long long rows, cudaStream_t s)
     while (N2 < b.maxT - 1)
         N2 <<= 1;
     const int    nbin = N2 <= 8192 ? (N2 < 4096 ? N2 : 4096) : 0;
-    const size_t smem = (size_t)N2 * 8 + (size_t)nbin * 8;
+    const size_t smem = (size_t)N2 * 8 + (size_t)rows_skewed(nbin) * 8;
+    // distances kept in registers up to 32 per thread (rows up to 8192)
+    const int N = b.maxT - 1;
+    void (*kernel)(WalkBatch) = N <= 8 * kRowsThreads    ? ksg_rows_kernel<8>
+                                : N <= 16 * kRowsThreads ? ksg_rows_kernel<16>
+                                : N <= 32 * kRowsThreads ? ksg_rows_kernel<32>
+                                                         : ksg_rows_kernel<0>;
     // static shared memory comes on top of the dynamic part: always raise
     // the limit to what this launch needs
-    cudaError_t e = cudaFuncSetAttribute(ksg_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;
-    ksg_rows_kernel<<<(unsigned)rows, kRowsThreads, smem, s>>>(b);
+    kernel<<<(unsigned)rows, kRowsThreads, smem, s>>>(b);
     return cudaGetLastError();
 }
 

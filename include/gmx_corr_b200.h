@@ -283,7 +283,9 @@ typedef struct gc_screen_report
     double audit_max_dr;   /* max |r_hat - r_ksg| over audit_accepted pairs */
     double audit_rms_dr;   /* rms of the same */
     double final_max_dr;   /* max |r_out - r_ksg| over the audit sample */
-    float  ms_features, ms_mlp, ms_ksg; /* device time of each stage */
+    /* device time of each stage; when at least half of the pairs are exact,
+       ms_ksg is the host time of one whole-matrix gc_ksg_matrix call */
+    float  ms_features, ms_mlp, ms_ksg;
 } gc_screen_report;
 
 void gc_screen_opts_init(gc_screen_opts* o);

@@ -21,51 +21,112 @@
 
 namespace gc {
 
-// One thread per component c = atom*3 + dim; sequential sums in frame
-// order with round-to-nearest intrinsics so no FMA contraction alters a
-// bit relative to the reference's plain double arithmetic.
-__global__ void ksg_prepare_kernel(const double* __restrict__ xyz, int natoms, int T,
-                                   double* __restrict__ X, int* __restrict__ status)
+// One CTA per atom, its three components side by side.  The mean and the
+// variance are sequential FP64 sums in frame order (one thread per
+// component, over chunks of the atom's frames staged in shared memory by
+// coalesced loads) with round-to-nearest intrinsics, so no FMA contraction
+// or reordering alters a bit relative to the reference's plain double
+// arithmetic.  The z-scores, their minimum (an exact operation in any
+// order) and the shifted rows are then computed by all threads.
+constexpr int kPrepThreads = 192; // a multiple of 3: thread e keeps component e % 3
+constexpr int kPrepChunk   = 512; // frames per staged chunk
+
+__global__ void __launch_bounds__(kPrepThreads) ksg_prepare_kernel(const double* __restrict__ xyz, int natoms, int T,
+                                                                   double* __restrict__ X, int* __restrict__ status)
 {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= natoms * 3)
-        return;
-    const int     atom = c / 3, d = c - 3 * (c / 3);
-    const double* src  = xyz + (size_t)atom * T * 3 + d;
-    double        me   = 0.0;
-    for (int f = 0; f < T; ++f)
-        me = __dadd_rn(me, src[(size_t)f * 3]);
-    me       = __ddiv_rn(me, (double)T);
-    double s = 0.0;
-    for (int f = 0; f < T; ++f)
+    __shared__ double buf[kPrepChunk * 3];
+    __shared__ double s_me[3], s_sd[3], s_mn[kPrepThreads / 32][3];
+    __shared__ int    s_bad;
+    const int         atom = blockIdx.x, tid = threadIdx.x;
+    const double*     src  = xyz + (size_t)atom * T * 3;
+    if (tid == 0)
+        s_bad = 0;
+    // pass 1: the mean, pass 2: the sum of squared deviations
+    for (int pass = 0; pass < 2; ++pass)
     {
-        const double t = __dsub_rn(src[(size_t)f * 3], me);
-        s              = __dadd_rn(s, __dmul_rn(t, t));
+        const double me  = pass ? s_me[tid < 3 ? tid : 0] : 0.0;
+        double       acc = 0.0;
+        for (int f0 = 0; f0 < T; f0 += kPrepChunk)
+        {
+            const int n = min(kPrepChunk, T - f0);
+            __syncthreads(); // the previous chunk is consumed
+            for (int e = tid; e < n * 3; e += kPrepThreads)
+                buf[e] = src[(size_t)f0 * 3 + e];
+            __syncthreads();
+            if (tid < 3)
+            {
+                if (pass == 0)
+                {
+#pragma unroll 8
+                    for (int f = 0; f < n; ++f)
+                        acc = __dadd_rn(acc, buf[f * 3 + tid]);
+                }
+                else
+                {
+#pragma unroll 8
+                    for (int f = 0; f < n; ++f)
+                    {
+                        const double t = __dsub_rn(buf[f * 3 + tid], me);
+                        acc            = __dadd_rn(acc, __dmul_rn(t, t));
+                    }
+                }
+            }
+        }
+        if (tid < 3)
+        {
+            if (pass == 0)
+                s_me[tid] = __ddiv_rn(acc, (double)T);
+            else
+            {
+                const double sd = __dsqrt_rn(__ddiv_rn(acc, (double)(T - 1)));
+                s_sd[tid]       = sd;
+                if (!isfinite(sd))
+                {
+                    atomicOr(status, kStatNonFinite);
+                    s_bad = 1;
+                }
+                else if (sd == 0.0)
+                {
+                    atomicOr(status, kStatZeroVariance);
+                    s_bad = 1;
+                }
+            }
+        }
+        __syncthreads();
     }
-    s = __ddiv_rn(s, (double)(T - 1));
-    s = __dsqrt_rn(s);
-    if (!isfinite(s))
-    {
-        atomicOr(status, kStatNonFinite);
+    if (s_bad)
         return;
-    }
-    if (s == 0.0)
+    // pass 3: minimum z per component (seeded like the reference's DBL_MAX/2
+    // with its integer DBL_MAX); pass 4: the rows z - min
+    const int    d  = tid % 3;
+    const double me = s_me[d], sd = s_sd[d];
+    double       mn = 1000000.0;
+    for (int e = tid; e < T * 3; e += kPrepThreads)
     {
-        atomicOr(status, kStatZeroVariance);
-        return;
-    }
-    // min/max seeds of the reference: DBL_MAX/2 with its integer DBL_MAX.
-    double  mn = 1000000.0, mx = -1000000.0;
-    double* row = X + (size_t)c * T;
-    for (int f = 0; f < T; ++f)
-    {
-        const double z = __ddiv_rn(__dsub_rn(src[(size_t)f * 3], me), s);
-        row[f]         = z;
+        const double z = __ddiv_rn(__dsub_rn(src[e], me), sd);
         mn             = z < mn ? z : mn;
-        mx             = z > mx ? z : mx;
     }
-    for (int f = 0; f < T; ++f)
-        row[f] = __dsub_rn(row[f], mn);
+    // lanes of a warp hold components (lane + 32 * warp) % 3; reduce per component
+    const int lane = tid & 31, warp = tid >> 5;
+    for (int c = 0; c < 3; ++c)
+    {
+        double v = d == c ? mn : 1000000.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            const double w = __shfl_xor_sync(0xFFFFFFFFu, v, o);
+            v              = w < v ? w : v;
+        }
+        if (lane == 0)
+            s_mn[warp][c] = v;
+    }
+    __syncthreads();
+    double mnd = s_mn[0][d];
+    for (int w = 1; w < kPrepThreads / 32; ++w)
+        mnd = s_mn[w][d] < mnd ? s_mn[w][d] : mnd;
+    double* row = X + (size_t)(atom * 3 + d) * T;
+    for (int e = tid; e < T * 3; e += kPrepThreads)
+        row[e / 3] = __dsub_rn(__ddiv_rn(__dsub_rn(src[e], me), sd), mnd);
 }
 
 namespace {
@@ -125,8 +186,7 @@ __global__ void ksg_finalize_kernel(const uint32_t* __restrict__ cnt, long pair_
 
 void launch_ksg_prepare(const double* xyz, int natoms, int T, double* X, int* status, cudaStream_t s)
 {
-    const int n = natoms * 3;
-    ksg_prepare_kernel<<<(n + 127) / 128, 128, 0, s>>>(xyz, natoms, T, X, status);
+    ksg_prepare_kernel<<<natoms, kPrepThreads, 0, s>>>(xyz, natoms, T, X, status);
 }
 
 void launch_ksg_exact(const double* X, int T, int K, long pair_begin, long pair_count, uint32_t* cnt,

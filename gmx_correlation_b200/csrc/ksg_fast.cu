@@ -1201,6 +1201,8 @@ __global__ void __launch_bounds__(256) ksg_fixup_kernel(WalkBatch B)
     for (int d = 0; d < B.n; ++d)
     {
         const WalkParams& p = B.d[d];
+        if (p.hq && *p.hq_len <= p.hq_cap) // every hand-over was queued (and is done)
+            continue;
         const long long   n = (long long)p.T * p.pair_count;
         for (long long c0 = ((long long)blockIdx.x * 8 + warp) * 32; c0 < n; c0 += (long long)gridDim.x * 8 * 32)
         {

@@ -173,8 +173,25 @@ __global__ void ksg_finalize_kernel(const uint32_t* __restrict__ cnt, long pair_
     const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (p >= pair_count)
         return;
+    // 16 frames' counts and digamma terms are fetched together; the sum
+    // itself stays sequential in frame order
     double s = 0.0;
-    for (int i = 0; i < T; ++i)
+    int    i = 0;
+    for (; i + 16 <= T; i += 16)
+    {
+        uint32_t c[16];
+        double   term[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u)
+            c[u] = cnt[(size_t)(i + u) * pair_count + p];
+#pragma unroll
+        for (int u = 0; u < 16; ++u)
+            term[u] = __dadd_rn(psi[c[u] & 0xFFFFu], psi[c[u] >> 16]);
+#pragma unroll
+        for (int u = 0; u < 16; ++u)
+            s = __dadd_rn(s, term[u]);
+    }
+    for (; i < T; ++i)
     {
         const uint32_t c = cnt[(size_t)i * pair_count + p];
         s                = __dadd_rn(s, __dadd_rn(psi[c & 0xFFFFu], psi[c >> 16]));

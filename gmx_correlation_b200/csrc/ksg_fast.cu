@@ -151,8 +151,9 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
     const float4  q   = xr[i];
     auto          frame_of = [i](int m) { return m < i ? m : m + 1; };
 
-    // the row's distances, entry m = tid + k * threads
+    // the row's distances (and later their buckets), entry m = tid + k * threads
     float dreg[R > 0 ? R : 1];
+    int   breg[R > 0 ? R : 1];
     if constexpr (R > 0)
     {
 #pragma unroll
@@ -170,18 +171,18 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
             {
                 const int m = tid + k * kRowsThreads;
                 if (m < N)
-                    fn(m, dreg[k]);
+                    fn(k, m, dreg[k]);
             }
         }
         else
         {
             for (int m = tid; m < N; m += kRowsThreads)
-                fn(m, dist3f(q, xr[frame_of(m)]));
+                fn(0, m, dist3f(q, xr[frame_of(m)]));
         }
     };
 
     unsigned kmin = 0xFFFFFFFFu, kmax = 0u;
-    each([&](int, float d) {
+    each([&](int, int, float d) {
         const unsigned k = __float_as_uint(d);
         kmin             = min(kmin, k);
         kmax             = max(kmax, k);
@@ -226,7 +227,7 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
         return c;
     };
     if (nbin)
-        each([&](int, float d) {
+        each([&](int, int, float d) {
             float f;
             atomicAdd(&coarse[warp][coarse_of(d, f)], 1u);
         });
@@ -264,7 +265,12 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
     };
     // histogram
     if (nbin)
-        each([&](int, float d) { atomicAdd(&hist[bin_of(d)], 1u); });
+        each([&](int slot, int, float d) {
+            const int b = bin_of(d);
+            if constexpr (R > 0)
+                breg[slot] = b;
+            atomicAdd(&hist[b], 1u);
+        });
     __syncthreads();
     // exclusive scan of hist into cursor (each thread a contiguous slice)
     const int per = nbin / kRowsThreads; // 0 without a bucket pass
@@ -298,11 +304,19 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
     __syncthreads();
     // scatter (or place in frame order for the bitonic network)
     const bool bucketed = !crowded;
-    each([&](int m, float d) {
+    each([&](int slot, int m, float d) {
         const int                j   = frame_of(m);
-        const unsigned long long k   = ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)j;
-        const unsigned           pos = bucketed ? atomicAdd(&cursor[bin_of(d)], 1u) : (unsigned)m;
-        keys[pos]                    = k;
+        const unsigned long long key = ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)j;
+        int                      b   = 0;
+        if (bucketed)
+        {
+            if constexpr (R > 0)
+                b = breg[slot];
+            else
+                b = bin_of(d);
+        }
+        const unsigned pos = bucketed ? atomicAdd(&cursor[b], 1u) : (unsigned)m;
+        keys[pos]          = key;
     });
     __syncthreads();
     if (bucketed)

@@ -89,6 +89,36 @@ def test_fast_path_reference_size(gc):
     exact.close()
 
 
+@pytest.mark.parametrize("n,T,k", [
+    (6, 3000, 100),   # rows of 2999 entries: 16 register slots per thread in the row sort
+    (5, 5000, 50),    # 4999 entries: 32 slots; coordinate rows too long to stage
+    (4, 9000, 100),   # 8999 entries: beyond the bucket pass, bitonic row sort
+    (10, 1200, 300),  # k >= 256: entries below the lower bound counted apart from the histogram
+])
+def test_fast_path_long_rows_and_large_k(gc, n, T, k):
+    """The fast path's row-length and k variants agree with the exact FP64
+    kernels on every pair."""
+    torch = pytest.importorskip("torch")
+    from gmx_correlation_b200.synth import synth_traj
+    x = synth_traj(n, T, 4, 0.08, seed=n + T + k, fp32=True)
+    d_xyz = torch.from_numpy(x).cuda()
+    fast = gc.KsgPlan(n, T, k)
+    exact = gc.KsgPlan(n, T, k, path=gc.PATH_EXACT_FP64)
+    assert fast.is_fast
+    out_f = torch.zeros(fast.pairs, dtype=torch.float64, device="cuda")
+    out_e = torch.zeros_like(out_f)
+    s = torch.cuda.Stream()
+    fast.run(d_xyz.data_ptr(), out_f.data_ptr(), s.cuda_stream)
+    exact.run(d_xyz.data_ptr(), out_e.data_ptr(), s.cuda_stream)
+    torch.cuda.synchronize()
+    fast.sync()
+    exact.sync()
+    assert fast.handoffs < 0.05 * fast.pairs * T, fast.handoff_reasons
+    np.testing.assert_array_equal(out_f.cpu().numpy(), out_e.cpu().numpy())
+    fast.close()
+    exact.close()
+
+
 def test_shard_equals_full(gc, small_x):
     full = gc.kraskov_corrmatrix(small_x, 10)
     part = gc.kraskov_corrmatrix(small_x, 10, pairs=(100, 777))

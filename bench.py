@@ -14,6 +14,10 @@ pair MI inside the timed region).  With N > 1 (torchrun, one rank per GPU)
 every rank processes its own independent trajectory (weak scaling, no
 data-path collective); timing is max over ranks.
 
+The cpu_baseline object also carries `legacy_gpu`: the reference's own
+legacy CUDA KSG kernel (lib/kraskov_gpu.cu, built for sm_100a into
+oracle/_ref) timed on a 64-atom slice of the workload.
+
 --impl reference times the reference's own OpenMP CPU implementation
 (oracle/_ref, the unmodified lib/*.cpp compiled here) on a bounded random
 sample of pairs of the same workload per step, with every host thread.
@@ -135,6 +139,51 @@ def cpu_baseline_sample(x, k, seconds: float, seed: int = 7):
     return {"value": m / dt, "unit": UNIT, "cores": threads, "kind": "reference",
             "sample": f"{m} random pairs of the 247x2000 k=100 matrix through the reference's "
                       f"kraskov_prepare+kraskov_wrap OpenMP loop ({dt:.1f} s)"}
+
+
+_LEGACY_GPU = r"""
+import ctypes, json, sys, time
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from gmx_correlation_b200.synth import CONFIGS, synth_traj
+c = CONFIGS["ref"]
+L = ctypes.CDLL(sys.argv[2])
+L.gcref_last_error.restype = ctypes.c_char_p
+dp = ctypes.POINTER(ctypes.c_double)
+def run(n, T, k, seed):
+    x = np.ascontiguousarray(synth_traj(n, T, c["n_modes"], c["sigma_l"], seed=seed, fp32=c["fp32"]))
+    m = np.zeros((n, n))
+    t0 = time.perf_counter()
+    if L.gcref_ksg_matrix_legacy_gpu(x.ctypes.data_as(dp), n, T, k, m.ctypes.data_as(dp)):
+        raise SystemExit(L.gcref_last_error().decode())
+    return time.perf_counter() - t0
+run(4, 200, 10, 1)  # CUDA context and module load, untimed
+n = int(sys.argv[3])
+dt = run(n, c["nframes"], c["k"], c["seed"])
+print(json.dumps({"value": n * (n - 1) / 2 / dt, "seconds": dt, "pairs": n * (n - 1) // 2}))
+"""
+
+
+def legacy_gpu_sample(natoms: int = 64):
+    """The reference's legacy CUDA KSG (lib/kraskov_gpu.cu, one block per pair,
+    brute force in FP64) built for sm_100a, through kraskov_corrmatrix_gpu on
+    a 64-atom slice of the workload (same frames and k, 2016 pairs), host time
+    around the call after an untimed warm-up call.  It runs in a child process
+    because the legacy host code exits the process on a CUDA error."""
+    so = ROOT / "oracle" / "_ref" / "libgcrefgpu.so"
+    if not so.exists():
+        return {"unavailable": "oracle/_ref/libgcrefgpu.so not built"}
+    try:
+        r = subprocess.run([sys.executable, "-c", _LEGACY_GPU, str(ROOT), str(so), str(natoms)],
+                           capture_output=True, text=True, timeout=300)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "legacy GPU KSG did not finish within 300 s"}
+    if r.returncode != 0:
+        return {"unavailable": (r.stderr or r.stdout).strip().splitlines()[-1:] or ["failed"]}
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    return {"value": d["value"], "unit": UNIT, "kind": "reference",
+            "sample": f"{d['pairs']} pairs ({natoms} atoms x 2000 frames, k=100) through the reference's "
+                      f"kraskov_corrmatrix_gpu, lib/kraskov_gpu.cu built for sm_100a ({d['seconds']:.2f} s)"}
 
 
 def run_reference(args):
@@ -337,6 +386,7 @@ def run_ours(args):
         if ws == 1 and not args.no_cpu_baseline:
             try:
                 out["cpu_baseline"] = cpu_baseline_sample(x, k, args.cpu_seconds)
+                out["cpu_baseline"]["legacy_gpu"] = legacy_gpu_sample()
             except Exception as e:  # noqa: BLE001
                 out["cpu_baseline"] = {"unavailable": str(e)}
         print(json.dumps(out))

@@ -29,7 +29,7 @@ _ip = ctypes.POINTER(ctypes.c_int)
 
 def build(ref: bool = True) -> None:
     """Compile the restatement, and the reference when its sources exist."""
-    targets = ["oracle"] + (["ref"] if ref and (REF_SRC / "lib").is_dir() else [])
+    targets = ["oracle"] + (["ref", "refgpu"] if ref and (REF_SRC / "lib").is_dir() else [])
     subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REF_SRC}", *targets], check=True)
 
 

@@ -16,7 +16,11 @@
 #include "correlation_core.h"
 #include "gcmi.h"
 #include "transfer_entropy.h"
+#ifdef GMX_CORRELATION_USE_CUDA
+#include "kraskov_gpu.h"
+#endif
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -285,5 +289,30 @@ int gcref_ksg_pair_detail(const double* xyz, int natoms, int nframes, int k, int
     done_traj(&t);
     return 0;
 }
+
+#ifdef GMX_CORRELATION_USE_CUDA
+// The reference's legacy CUDA KSG (lib/kraskov_gpu.cu, kraskov_mi_kernel),
+// reached the way kraskov_corrmatrix(use_gpu = true) reaches it
+// (lib/correlation_core.cpp:331-347) but without its silent CPU fallback:
+// k > 128 or no CUDA device is an error here.  Only in libgcrefgpu.so.
+int gcref_ksg_matrix_legacy_gpu(const double* xyz, int natoms, int nframes, int k, double* mat)
+{
+    if (k > 128 || !kraskov_gpu_probe())
+    {
+        g_err = "legacy GPU KSG unavailable: k > 128 or no CUDA device";
+        return 1;
+    }
+    t_traj t  = make_traj(xyz, natoms, nframes);
+    int    rc = guarded([&] {
+        std::fill(mat, mat + (size_t)natoms * natoms, 0.0);
+        t_kraskov kr;
+        kraskov_prepare(&t, &kr);
+        kraskov_corrmatrix_gpu(&kr, natoms, mat, k);
+        kraskov_done(&kr);
+    });
+    done_traj(&t);
+    return rc;
+}
+#endif
 
 } // extern "C"

@@ -11,8 +11,8 @@
 //                     |d32 - d64| <= eps_a for every marginal distance.
 //   ksg_rows_kernel   per (atom, query): the T-1 marginal distances, sorted
 //                     ascending, with their frame indices (S rows, P rows).
-//   ksg_walk_kernel   one pair and 32 consecutive queries per warp, one
-//                     query per lane.  Each lane walks the sorted row of the
+//   ksg_walk_kernel   one pair per CTA task, 32 consecutive queries per warp,
+//                     one query per lane.  Each lane walks the sorted row of the
 //                     marginal whose k-th distance is larger, gathering the
 //                     other marginal, and histograms the joint distances in
 //                     its own shared-memory column (anchored at the exact
@@ -517,10 +517,11 @@ __device__ __forceinline__ LaneSetup lane_setup(const WalkParams& p, int a1, int
     return u;
 }
 
-// CTA task t of a query block: chunk c of (warps per CTA) query groups of 32
-// consecutive queries, one group per warp, for the pair pair_order[k]
-// (pairs in atom-tile order, so the rows the running tasks read stay in L2).
-// Every thread of the CTA calls this; it ends with a barrier.
+// CTA task t of a query block: chunk c of B.chunk query groups of 32
+// consecutive queries, which the CTA's warps take one group at a time, for
+// the pair pair_order[k] (pairs in atom-tile order, so the rows the running
+// tasks read stay in L2).  Every thread of the CTA calls next_task; it ends
+// with a barrier.
 struct Task
 {
     int  c;

@@ -63,7 +63,10 @@ __device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v)
 // (no element storage).  top_shift is the bit offset of the most
 // significant byte that can be non-zero (56 for IEEE doubles).  Returns the
 // key; *below gets the number of elements with a strictly smaller key.
-// Every lane returns the same values.
+// Once the chosen byte bucket holds a single element, that element is the
+// answer and one more pass reads it (distinct distances usually end the
+// selection after the third of eight bytes).  Every lane returns the same
+// values.
 template <class KeyFn>
 __device__ unsigned long long warp_select_u64(KeyFn&& key, int n, int k, int top_shift,
                                               unsigned* hist, int lane, int* below)
@@ -104,7 +107,7 @@ __device__ unsigned long long warp_select_u64(KeyFn&& key, int n, int k, int top
         const bool     here  = excl < (unsigned)krem && (unsigned)krem <= incl;
         const unsigned owner = __ballot_sync(kFull, here);
         int            digit = 0;
-        unsigned       bel   = 0;
+        unsigned       bel = 0, cnt = 0;
         if (here)
         {
             unsigned acc = excl;
@@ -115,6 +118,7 @@ __device__ unsigned long long warp_select_u64(KeyFn&& key, int n, int k, int top
                 {
                     digit = lane * 8 + b;
                     bel   = acc;
+                    cnt   = c[b];
                     break;
                 }
                 acc += c[b];
@@ -123,9 +127,27 @@ __device__ unsigned long long warp_select_u64(KeyFn&& key, int n, int k, int top
         const int src = owner ? __ffs(owner) - 1 : 0;
         digit         = __shfl_sync(kFull, digit, src);
         bel           = __shfl_sync(kFull, bel, src);
+        cnt           = __shfl_sync(kFull, cnt, src);
         krem -= (int)bel;
         prefix |= (unsigned long long)digit << shift;
         mask |= 0xFFull << shift;
+        if (cnt == 1u && shift > 0)
+        {
+            // a single candidate carries this prefix: it is the k-th key (so
+            // it is untied, and krem == 1); one more pass reads it whole
+            unsigned long long found = 0ull;
+            for (int j = lane; j < n; j += 32)
+            {
+                unsigned long long kv;
+                if (key(j, kv) && (kv & mask) == prefix)
+                    found = kv;
+            }
+            const unsigned hi = __reduce_or_sync(kFull, (unsigned)(found >> 32));
+            const unsigned lo = __reduce_or_sync(kFull, (unsigned)found);
+            __syncwarp();
+            *below = k - krem;
+            return ((unsigned long long)hi << 32) | lo;
+        }
         __syncwarp();
     }
     *below = k - krem;

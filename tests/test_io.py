@@ -1,6 +1,11 @@
 """Output contract: pearsify and the correl.dat / XPM writers of the product
 library (host code, no GPU needed) against the reference's own output."""
+import importlib.util
+import warnings
+from pathlib import Path
+
 import numpy as np
+import pytest
 
 from tests.conftest import GOLDEN
 
@@ -49,3 +54,31 @@ def test_writer_bad_path(gc):
     import pytest
     with pytest.raises(gc.GCError):
         gc.write_matrix(np.eye(2), "/nonexistent-dir/x.dat")
+
+
+REF_CONSUMER = Path("/root/reference/bin/analyze_matrix.py")
+
+
+@pytest.mark.skipif(not REF_CONSUMER.exists(), reason="reference sources not present")
+def test_reference_consumer_reads_our_correl_dat(gc, tmp_path):
+    """The reference's downstream consumer (bin/analyze_matrix.py:71-102
+    read_matrix, :173-190 auto_threshold) reads the correl.dat this library
+    writes back to the same matrix, to the writer's %10.6g precision."""
+    spec = importlib.util.spec_from_file_location("ref_analyze_matrix", REF_CONSUMER)
+    mod = importlib.util.module_from_spec(spec)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")  # its optional plotting/graph imports
+        spec.loader.exec_module(mod)
+    rng = np.random.default_rng(5)
+    m = rng.random((31, 31))
+    m = 0.5 * (m + m.T)
+    m[np.diag_indices(31)] = 2000.0
+    gc.pearsify(m, 3)
+    out = tmp_path / "correl.dat"
+    gc.write_matrix(m, out)
+    theirs = mod.read_matrix(out)
+    np.testing.assert_array_equal(theirs, gc.read_matrix(out))
+    np.testing.assert_allclose(theirs, m, rtol=1e-5, atol=1e-6)
+    iu = np.triu_indices(31, 1)
+    vals = theirs[iu][theirs[iu] > 0]
+    assert mod.auto_threshold(theirs) == pytest.approx(float(vals.mean() + 0.5 * vals.std()), rel=1e-12)

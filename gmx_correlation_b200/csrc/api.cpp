@@ -559,6 +559,8 @@ gc_status gc_te_matrix(const gc_traj_view* traj, int k, int lag, const gc_opts* 
     DevBuf<double>    d_xyz, d_XT, d_psi, d_te;
     DevBuf<uint2>     d_cnt;
     DevBuf<int>       d_st;
+    DevBuf<float4>    d_X32;
+    DevBuf<float>     d_eps;
     GC_TRY(d_xyz.alloc((size_t)n * T * 3));
     GC_TRY(d_XT.alloc((size_t)n * T * 3));
     GC_TRY(d_psi.alloc((size_t)Nv + 1));
@@ -571,7 +573,15 @@ gc_status gc_te_matrix(const gc_traj_view* traj, int k, int lag, const gc_opts* 
     GC_TRY_CUDA(cudaMemsetAsync(d_st.p, 0, sizeof(int), ss.s));
     GC_TRY_CUDA(cudaMemsetAsync(d_te.p, 0, sizeof(double) * (size_t)n * n, ss.s));
     gc::launch_transpose_components(d_xyz.p, n, T, d_XT.p, d_st.p, ss.s);
-    gc::launch_te_exact(d_XT.p, n, T, k, lag, d_cnt.p, ss.s);
+    if (o.path == GC_PATH_EXACT_FP64)
+        gc::launch_te_exact(d_XT.p, n, T, k, lag, d_cnt.p, ss.s);
+    else
+    {
+        GC_TRY(d_X32.alloc((size_t)n * T));
+        GC_TRY(d_eps.alloc((size_t)n));
+        gc::launch_te_x32(d_XT.p, n, T, d_X32.p, d_eps.p, ss.s);
+        gc::launch_te_fast(d_XT.p, d_X32.p, d_eps.p, n, T, k, lag, d_cnt.p, ss.s);
+    }
     gc::launch_te_finalize(d_cnt.p, n, T, k, lag, d_psi.p, d_te.p, ss.s);
     GC_TRY_CUDA(cudaGetLastError());
     GC_TRY_CUDA(cudaStreamSynchronize(ss.s));

@@ -45,6 +45,11 @@ void launch_transpose_components(const double* xyz, int natoms, int T, double* X
 // Exact FP64 TE statistics for every ordered pair; cnt[qi * npairs + q] =
 // {n_xp | n_xfxp << 16, n_ypxp}.
 void launch_te_exact(const double* XT, int natoms, int T, int K, int lag, uint2* cnt, cudaStream_t s);
+// FP32 copy of the raw coordinates and per-atom error bounds for launch_te_fast.
+void launch_te_x32(const double* XT, int natoms, int T, float4* X32, float* eps_atom, cudaStream_t s);
+// TE statistics from FP32 distances with exact FP64 repair (same counts as launch_te_exact).
+void launch_te_fast(const double* XT, const float4* X32, const float* eps_atom, int natoms, int T, int K, int lag,
+                    uint2* cnt, cudaStream_t s);
 // TE per ordered pair q = a1*(natoms-1) + (a2 < a1 ? a2 : a2-1), into te[a1*n+a2].
 void launch_te_finalize(const uint2* cnt, int natoms, int T, int K, int lag, const double* psi,
                         double* te_mat, cudaStream_t s);

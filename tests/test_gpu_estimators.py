@@ -47,3 +47,20 @@ def test_te_too_few_frames_is_zero(gc):
     from gmx_correlation_b200.synth import synth_traj
     x = synth_traj(3, 12, 2, 0.1, seed=3)
     assert not gc.te_matrix(x, 10, 5).any()
+
+
+@pytest.mark.parametrize("n,T,k,lag,grid", [
+    (12, 900, 20, 1, 0.0),
+    (9, 1500, 100, 5, 0.0),
+    (8, 500, 10, 2, 0.02),   # coordinates on a 0.02 nm grid: exact distance ties at eps
+])
+def test_te_fast_path_equals_exact(gc, n, T, k, lag, grid):
+    """The FP32 TE kernel with FP64 repair gives the exact kernel's matrix,
+    bit for bit, also when many distances tie at eps."""
+    from gmx_correlation_b200.synth import synth_traj
+    x = synth_traj(n, T, 4, 0.08, seed=n * T + k)
+    if grid:
+        x = np.round(x / grid) * grid
+    fast = gc.te_matrix(x, k, lag)
+    exact = gc.te_matrix(x, k, lag, path=gc.PATH_EXACT_FP64)
+    np.testing.assert_array_equal(fast, exact)

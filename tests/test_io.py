@@ -56,7 +56,9 @@ def test_writer_bad_path(gc):
         gc.write_matrix(np.eye(2), "/nonexistent-dir/x.dat")
 
 
-REF_CONSUMER = Path("/root/reference/bin/analyze_matrix.py")
+from oracle import REF_SRC  # noqa: E402
+
+REF_CONSUMER = REF_SRC / "bin" / "analyze_matrix.py"
 
 
 @pytest.mark.skipif(not REF_CONSUMER.exists(), reason="reference sources not present")

@@ -758,7 +758,7 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
             const int reason = (wrap > 255u || (LO && bstar == 0)) ? kReasonBand
                                : (bstar >= (int)kTop ? kReasonRange : 0);
             // the result names buckets from L (index - 1 under LO)
-            p.wres[(size_t)iq * p.pair_count + tk.pl] = pack_walk(LO ? bstar - 1 : bstar, prefix, m_end, reason);
+            p.wres[(size_t)tk.pl * p.Q + iq] = pack_walk(LO ? bstar - 1 : bstar, prefix, m_end, reason);
         }
         if (p.walk_elems)
         {
@@ -819,7 +819,7 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
         {
             const int                a1 = tk.a1, a2 = tk.a2;
             const int                i  = p.i0 + iq;
-            const unsigned long long wr = p.wres[(size_t)iq * p.pair_count + tk.pl];
+            const unsigned long long wr = p.wres[(size_t)tk.pl * p.Q + iq];
             const int                bstar = (int)(wr & 0xFF), prefix = (int)((wr >> 8) & 0xFFFF);
             const int                m_end = (int)((wr >> 24) & 0xFFFF);
             int                      reason = (int)((wr >> 40) & 0xFF);

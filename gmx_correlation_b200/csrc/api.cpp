@@ -506,7 +506,7 @@ gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, do
         for (long pl = 0; pl < pc; ++pl)
             for (int i = 0; i < T; ++i)
             {
-                const uint32_t v = c[(size_t)i * pc + pl];
+                const uint32_t v = c[(size_t)pl * T + i];
                 if (o.detail_nx)
                     o.detail_nx[(size_t)pl * T + i] = (int32_t)(v & 0xFFFFu);
                 if (o.detail_ny)

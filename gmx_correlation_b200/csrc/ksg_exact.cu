@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kExactWarps * 32)
     {
         const uint32_t c = exact_query(X, T, K, a1, a2, i, box, rank_shift, hist[warp], lane);
         if (lane == 0)
-            cnt[(size_t)i * pair_count + pl] = c;
+            cnt[(size_t)pl * T + i] = c;
     }
 }
 
@@ -183,7 +183,7 @@ __global__ void ksg_finalize_kernel(const uint32_t* __restrict__ cnt, long pair_
         double   term[16];
 #pragma unroll
         for (int u = 0; u < 16; ++u)
-            c[u] = cnt[(size_t)(i + u) * pair_count + p];
+            c[u] = cnt[(size_t)p * T + i + u];
 #pragma unroll
         for (int u = 0; u < 16; ++u)
             term[u] = __dadd_rn(psi[c[u] & 0xFFFFu], psi[c[u] >> 16]);
@@ -193,7 +193,7 @@ __global__ void ksg_finalize_kernel(const uint32_t* __restrict__ cnt, long pair_
     }
     for (; i < T; ++i)
     {
-        const uint32_t c = cnt[(size_t)i * pair_count + p];
+        const uint32_t c = cnt[(size_t)p * T + i];
         s                = __dadd_rn(s, __dadd_rn(psi[c & 0xFFFFu], psi[c >> 16]));
     }
     const double phiK = __dsub_rn(psi[K], __ddiv_rn(1.0, (double)K));

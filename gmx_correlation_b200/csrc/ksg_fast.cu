@@ -1164,10 +1164,10 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
                 {
                     const unsigned q = atomicAdd(p.hq_len, 1u);
                     if (q < p.hq_cap)
-                        p.hq[q] = (unsigned long long)i * p.pair_count + tk.pl;
+                        p.hq[q] = (unsigned long long)tk.pl * p.T + i;
                 }
             }
-            p.cnt[(size_t)i * p.pair_count + tk.pl] = out;
+            p.cnt[(size_t)tk.pl * p.T + i] = out;
         }
         __syncwarp(); // band columns of every lane are free for the next task
     }
@@ -1176,8 +1176,8 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
 // Exact FP64 statistics of one handed-over (query, pair): cnt index idx.
 __device__ __forceinline__ void fixup_one(const WalkParams& p, long long idx, unsigned* hist, int lane)
 {
-    const int  i  = (int)(idx / p.pair_count);
-    const long pl = (long)(idx - (long long)i * p.pair_count);
+    const long pl = (long)(idx / p.T);
+    const int  i  = (int)(idx - (long long)pl * p.T);
     int        a1, a2;
     if (p.pair_ab)
     {

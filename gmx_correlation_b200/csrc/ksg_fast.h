@@ -29,9 +29,9 @@ struct WalkParams
     const int2*     pair_ab;    // optional [pair_count] (a1, a2) of an explicit pair list
     const int*      pair_order; // optional task order: task k computes local pair pair_order[k]
     int             shift;      // histogram bucket = 2^shift float ulps above the lower bound
-    uint32_t*       cnt;        // [T][pair_count] n_x | n_y << 16, or kHandOver
+    uint32_t*       cnt;        // [pair_count][T] n_x | n_y << 16, or kHandOver
     unsigned long long* wres;   // [pair_count][Q] walk results of the block (a warp's 32 queries side by side)
-    unsigned long long* hq;     // hand-over queue: cnt indices i * pair_count + pl
+    unsigned long long* hq;     // hand-over queue: cnt indices pl * T + i
     unsigned*           hq_len;
     unsigned            hq_cap;
     int*                status;

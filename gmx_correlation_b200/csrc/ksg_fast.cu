@@ -940,7 +940,10 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
                             rk += u < v || (u == v && f < e);
                         }
                         if (rk == r - 1)
+                        {
                             d32 = v;
+                            break;
+                        }
                     }
                     lower             = __fsub_rd(d32, e2);
                     const float upper = __fadd_ru(d32, e2);

@@ -242,17 +242,17 @@ void remember_walk_config(int maxT, int k, const WalkConfig& cfg)
 
 std::vector<WalkConfig> walk_candidates(int maxT)
 {
+    // Measured on 247 x 2000 and 128 x 5000 matrices: fewer warps than the
+    // staged rows allow (24, 16, or two CTAs of 11-12 per SM) and chunks of
+    // one group per warp were always slower, so the search spans the atom
+    // tile and chunks of two or four groups per warp.
     std::vector<WalkConfig> out;
     const int               wmax = walk_max_staged_warps(maxT);
     std::vector<int>        warps;
     if (wmax > 0)
-    {
-        for (int w : {wmax, 24, 16})
-            if (w <= wmax && std::find(warps.begin(), warps.end(), w) == warps.end())
-                warps.push_back(w);
-    }
+        warps.push_back(wmax);
     for (int tile : {16, 32})
-        for (int mult : {1, 2, 4})
+        for (int mult : {2, 4})
         {
             if (warps.empty())
             {

@@ -106,22 +106,23 @@ __device__ __forceinline__ int batch_desc(const long long* __restrict__ prefix, 
 // key per bucket, which one thread per bucket insertion-sorts.  R > 0: each
 // thread keeps its R distances (entries tid + r * threads) in registers for
 // the passes; R = 0: distances are recomputed from the atom's coordinate row
-// (L1-resident) in every pass.  A row with a crowded bucket (more than 64
+// (L1-resident) in every pass.  THREADS (256 or 512) threads per row; 512
+// only for rows longer than 2048 entries, so every thread owns whole
+// buckets of the scan.  A row with a crowded bucket (more than 64
 // equal-ish distances, e.g. duplicated frames), and rows longer than 8192,
 // are sorted by a bitonic network instead.
-constexpr int kRowsThreads = 256;
 
 // Bucket counters and cursors carry one padding word per 32, so the
 // contiguous bucket slices a thread scans start in distinct banks.
 __device__ __forceinline__ int rows_skew(int b) { return b + (b >> 5); }
 __host__ __device__ constexpr int rows_skewed(int nbin) { return nbin + (nbin >> 5); }
 
-template <int R>
-__global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
+template <int THREADS, int R>
+__global__ void __launch_bounds__(THREADS) ksg_rows_kernel(WalkBatch B)
 {
     extern __shared__ __align__(16) unsigned char rows_smem[];
-    __shared__ unsigned red_min[kRowsThreads / 32], red_max[kRowsThreads / 32];
-    __shared__ unsigned coarse[kRowsThreads / 32][64];
+    __shared__ unsigned red_min[THREADS / 32], red_max[THREADS / 32];
+    __shared__ unsigned coarse[THREADS / 32][64];
     __shared__ float    cum[65];
     __shared__ int      crowded;
 
@@ -136,7 +137,7 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
     const int         i   = w.i0 + iq;
     const int         N   = T - 1;
     const int         tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    int               N2  = 256;
+    int               N2  = THREADS; // at least one bucket per thread in the scan
     while (N2 < N)
         N2 <<= 1;
     // bucket pass up to 8192 keys; longer rows use the bitonic network alone
@@ -159,7 +160,7 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
 #pragma unroll
         for (int k = 0; k < R; ++k)
         {
-            const int m = tid + k * kRowsThreads;
+            const int m = tid + k * THREADS;
             dreg[k]     = m < N ? dist3f(q, xr[frame_of(m)]) : 0.0f;
         }
     }
@@ -169,14 +170,14 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
 #pragma unroll
             for (int k = 0; k < R; ++k)
             {
-                const int m = tid + k * kRowsThreads;
+                const int m = tid + k * THREADS;
                 if (m < N)
                     fn(k, m, dreg[k]);
             }
         }
         else
         {
-            for (int m = tid; m < N; m += kRowsThreads)
+            for (int m = tid; m < N; m += THREADS)
                 fn(0, m, dist3f(q, xr[frame_of(m)]));
         }
     };
@@ -187,7 +188,7 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
         kmin             = min(kmin, k);
         kmax             = max(kmax, k);
     });
-    for (int b = tid; b < rows_skewed(nbin); b += kRowsThreads)
+    for (int b = tid; b < rows_skewed(nbin); b += THREADS)
         hist[b] = 0u;
     for (int e = lane; e < 64; e += 32)
         coarse[warp][e] = 0u;
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
     __syncthreads();
     kmin = red_min[0];
     kmax = red_max[0];
-    for (int w = 1; w < kRowsThreads / 32; ++w)
+    for (int w = 1; w < THREADS / 32; ++w)
     {
         kmin = min(kmin, red_min[w]);
         kmax = max(kmax, red_max[w]);
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
     {
         // exclusive prefix over the 64 coarse bins (two per lane), as floats
         unsigned c0 = 0u, c1 = 0u;
-        for (int w = 0; w < kRowsThreads / 32; ++w)
+        for (int w = 0; w < THREADS / 32; ++w)
         {
             c0 += coarse[w][2 * lane];
             c1 += coarse[w][2 * lane + 1];
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
         });
     __syncthreads();
     // exclusive scan of hist into cursor (each thread a contiguous slice)
-    const int per = nbin / kRowsThreads; // 0 without a bucket pass
+    const int per = nbin / THREADS; // 0 without a bucket pass
     unsigned  loc = 0;
     for (int e = 0; e < per; ++e)
         loc += hist[rows_skew(tid * per + e)];
@@ -324,7 +325,7 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
         // cursor[b] now holds the end of bucket b; sort each bucket (thread
         // t takes buckets t, t + threads, ..., so a warp's buckets, and
         // their keys, lie side by side)
-        for (int b = tid; b < nbin; b += kRowsThreads)
+        for (int b = tid; b < nbin; b += THREADS)
         {
             const int      bs  = rows_skew(b);
             const unsigned end = cursor[bs], beg = end - hist[bs];
@@ -344,13 +345,13 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
     }
     else
     {
-        for (int m = N + tid; m < N2; m += kRowsThreads)
+        for (int m = N + tid; m < N2; m += THREADS)
             keys[m] = ~0ull;
         __syncthreads();
         for (int k = 2; k <= N2; k <<= 1)
             for (int j = k >> 1; j > 0; j >>= 1)
             {
-                for (int t = tid; t < (N2 >> 1); t += kRowsThreads)
+                for (int t = tid; t < (N2 >> 1); t += THREADS)
                 {
                     const int                idx = ((t / j) * (j << 1)) + (t % j);
                     const int                prt = idx + j;
@@ -368,7 +369,7 @@ __global__ void __launch_bounds__(kRowsThreads) ksg_rows_kernel(WalkBatch B)
     // queries of a block side by side (see WalkParams)
     const size_t base    = ((size_t)a * (Lpad >> 2) * Qp + iq) * 4;
     const size_t gstride = (size_t)Qp * 4;
-    for (int m = tid; m < N; m += kRowsThreads)
+    for (int m = tid; m < N; m += THREADS)
     {
         const unsigned long long k   = keys[m];
         const size_t             idx = base + (size_t)(m >> 2) * gstride + (m & 3);
@@ -1251,18 +1252,30 @@ cudaError_t launch_ksg_rows(const WalkBatch& b, long long rows, cudaStream_t s)
         N2 <<= 1;
     const int    nbin = N2 <= 8192 ? (N2 < 4096 ? N2 : 4096) : 0;
     const size_t smem = (size_t)N2 * 8 + (size_t)rows_skewed(nbin) * 8;
-    // distances kept in registers up to 32 per thread (rows up to 8192)
-    const int N = b.maxT - 1;
-    void (*kernel)(WalkBatch) = N <= 8 * kRowsThreads    ? ksg_rows_kernel<8>
-                                : N <= 16 * kRowsThreads ? ksg_rows_kernel<16>
-                                : N <= 32 * kRowsThreads ? ksg_rows_kernel<32>
-                                                         : ksg_rows_kernel<0>;
+    // distances kept in registers, 8 per thread up to 2048 entries, then
+    // 512 threads with 8 or 16 each (measured faster than 256 threads with
+    // 16 or 32 at 4999 entries); longer rows recompute them
+    const int N       = b.maxT - 1;
+    int       threads = 256;
+    void (*kernel)(WalkBatch) = ksg_rows_kernel<256, 0>;
+    if (N <= 8 * 256)
+        kernel = ksg_rows_kernel<256, 8>;
+    else if (N <= 8 * 512)
+    {
+        kernel  = ksg_rows_kernel<512, 8>;
+        threads = 512;
+    }
+    else if (N <= 16 * 512)
+    {
+        kernel  = ksg_rows_kernel<512, 16>;
+        threads = 512;
+    }
     // static shared memory comes on top of the dynamic part: always raise
     // the limit to what this launch needs
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;
-    kernel<<<(unsigned)rows, kRowsThreads, smem, s>>>(b);
+    kernel<<<(unsigned)rows, threads, smem, s>>>(b);
     return cudaGetLastError();
 }
 

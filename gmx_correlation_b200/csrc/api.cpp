@@ -265,7 +265,8 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
     {
         const gc::host::WalkConfig cfg = gc::host::walk_config(nframes, k);
         GC_TRY(p->ft.create(natoms, nframes, k, pb, pc, o.pair_list, p->pair_ab.p,
-                            gc::host::ksg_block_queries(natoms, nframes, 8.0 * (1 << 30)), cfg.pair_tile));
+                            gc::host::ksg_block_queries(natoms, nframes, 16.0 * (1 << 30), 32 * cfg.walk_warps),
+                            cfg.pair_tile));
         std::vector<std::vector<gc::WalkParams>> waves;
         for (int b = 0; b < p->ft.blocks(); ++b)
             waves.push_back({p->ft.desc(p->X.p, p->cnt.p, p->status.p, b)});

@@ -14,13 +14,19 @@
 namespace gc {
 namespace host {
 
-int ksg_block_queries(int natoms, int T, double budget)
+int ksg_block_queries(int natoms, int T, double budget, int quantum)
 {
     const int    Lpad = ((T - 1) + 31) & ~31;
     const double row  = (double)natoms * Lpad * 6.0;
     long         q    = (long)(budget / row) / 32 * 32;
     q                 = q < 32 ? 32 : q;
-    return (int)(q > T ? T : q);
+    if (q >= T)
+        return T;
+    // whole rounds of the walk CTA's warps: a block of q queries gives each
+    // pair q / 32 query groups, which the CTA's warps take one at a time
+    if (quantum > 32 && q >= quantum)
+        q = q / quantum * quantum;
+    return (int)q;
 }
 
 gc_status KsgTraj::create(int n, int nframes, int k, long pb, long pc, const int64_t* lst, const int2* d_ab, int q,

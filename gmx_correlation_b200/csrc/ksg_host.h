@@ -53,8 +53,9 @@ struct KsgTraj
 };
 
 // Query-block size for one trajectory whose sorted rows of a block must fit
-// in budget bytes.
-int ksg_block_queries(int natoms, int T, double budget);
+// in budget bytes; when the trajectory needs several blocks, a multiple of
+// quantum queries if the budget allows one.
+int ksg_block_queries(int natoms, int T, double budget, int quantum = 32);
 
 // Device tables of a sequence of waves: each wave one launch of the row
 // sort, the walk and the finish over the descriptors of that wave; then one

@@ -60,18 +60,29 @@ int current_device()
 
 } // namespace
 
-void* gc::host::pool_take(size_t bytes)
+size_t gc::host::pool_round(size_t bytes)
+{
+    if (bytes <= ((size_t)2 << 20))
+        return (bytes + 255) & ~(size_t)255;
+    size_t step = (size_t)2 << 20;
+    while (step * 16 <= bytes)
+        step <<= 1; // an eighth to a sixteenth of the size
+    return (bytes + step - 1) / step * step;
+}
+
+void* gc::host::pool_take(size_t bytes, size_t* got)
 {
     const int d = current_device();
     if (d < 0)
         return nullptr;
     std::lock_guard<std::mutex> lock(g_pool_mutex);
-    auto                        it = g_pool[d].blocks.find(bytes);
-    if (it == g_pool[d].blocks.end())
+    auto                        it = g_pool[d].blocks.lower_bound(bytes);
+    if (it == g_pool[d].blocks.end() || it->first > bytes + bytes / 4)
         return nullptr;
     void* p = it->second;
+    *got    = it->first;
+    g_pool[d].bytes -= it->first;
     g_pool[d].blocks.erase(it);
-    g_pool[d].bytes -= bytes;
     return p;
 }
 

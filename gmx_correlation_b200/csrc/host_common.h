@@ -107,16 +107,23 @@ struct DevBuf
 // Per-device pool of large device blocks (exact-size reuse): plans of the
 // same shape created one after another reuse the blocks instead of calling
 // cudaMalloc / cudaFree.  pool_release frees every pooled block.
-void* pool_take(size_t bytes);             // a block of exactly `bytes`, or nullptr
-void  pool_give(void* p, size_t bytes);    // keeps the block (or frees it when the pool is full)
+// The smallest pooled block of at least `bytes` and at most 1.25 x `bytes`
+// (its size in *got), or nullptr.
+void*  pool_take(size_t bytes, size_t* got);
+void   pool_give(void* p, size_t bytes);   // keeps the block (or frees it when the pool is full)
+// Size of a fresh block for `bytes`: above 2 MiB rounded up to an eighth of
+// its power of two, so blocks of similar requests can be reused; below, to
+// 256 bytes.
+size_t pool_round(size_t bytes);
 void  pool_release();
 
 // DevBuf whose blocks come from and return to the pool.
 template <class T>
 struct PoolBuf
 {
-    T*     p = nullptr;
-    size_t n = 0;
+    T*     p   = nullptr;
+    size_t n   = 0;
+    size_t cap = 0; // bytes of the block
     PoolBuf() = default;
     PoolBuf(const PoolBuf&) = delete;
     PoolBuf& operator=(const PoolBuf&) = delete;
@@ -124,24 +131,27 @@ struct PoolBuf
     void reset()
     {
         if (p)
-            pool_give(p, n * sizeof(T));
-        p = nullptr;
-        n = 0;
+            pool_give(p, cap);
+        p   = nullptr;
+        n   = 0;
+        cap = 0;
     }
     gc_status alloc(size_t count)
     {
         reset();
         if (count == 0)
             count = 1;
-        void* q = pool_take(count * sizeof(T));
+        size_t got = 0;
+        void*  q   = pool_take(count * sizeof(T), &got);
         if (!q)
         {
-            cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+            got           = pool_round(count * sizeof(T));
+            cudaError_t e = cudaMalloc(&q, got);
             if (e == cudaErrorMemoryAllocation)
             {
                 cudaGetLastError();
                 pool_release(); // free what the pool holds and try once more
-                e = cudaMalloc(&q, count * sizeof(T));
+                e = cudaMalloc(&q, got);
             }
             if (e != cudaSuccess)
             {
@@ -150,8 +160,9 @@ struct PoolBuf
                             std::string("cudaMalloc: ") + cudaGetErrorString(e));
             }
         }
-        p = static_cast<T*>(q);
-        n = count;
+        p   = static_cast<T*>(q);
+        n   = count;
+        cap = got;
         return GC_OK;
     }
 };

@@ -70,12 +70,18 @@ std::mutex  g_batch_mutex;
 BatchPlan*  g_batch[64] = {};
 
 // Query-block size of every trajectory for the smallest number of waves
-// whose sorted rows fit the budget.
+// whose sorted rows fit the budget.  A trajectory split into several blocks
+// gets blocks of whole rounds of the walk CTA's warps (32 x warps queries),
+// so every warp has a query group in every round of a pair's task.
 std::vector<int> batch_blocks(const std::vector<std::unique_ptr<BatchTraj>>& t)
 {
     int maxT = 0;
     for (const auto& b : t)
         maxT = std::max(maxT, b->T);
+    int warps  = 0;
+    bool staged = false;
+    gc::walk_shape(maxT, &warps, &staged);
+    const int quantum = 32 * warps;
     for (int waves = 1;; ++waves)
     {
         std::vector<int> q;
@@ -83,7 +89,9 @@ std::vector<int> batch_blocks(const std::vector<std::unique_ptr<BatchTraj>>& t)
         for (const auto& b : t)
         {
             int Qb = ((b->T + waves - 1) / waves + 31) & ~31;
-            Qb     = std::min(Qb, b->T);
+            if (Qb < b->T && Qb > quantum)
+                Qb = (Qb + quantum - 1) / quantum * quantum;
+            Qb = std::min(Qb, b->T);
             q.push_back(Qb);
             bytes += (double)b->natoms * (((b->T - 1) + 31) & ~31) * ((Qb + 31) & ~31) * 6.0;
         }

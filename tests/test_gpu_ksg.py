@@ -119,6 +119,22 @@ def test_fast_path_long_rows_and_large_k(gc, n, T, k):
     exact.close()
 
 
+def test_fast_path_several_query_blocks(gc):
+    """600 atoms x 4000 frames needs its sorted rows in several query blocks
+    (blocks of 768 queries, the last one partial): listed pairs through the
+    fast path equal the exact FP64 kernels."""
+    from gmx_correlation_b200.synth import synth_traj
+    x = synth_traj(600, 4000, 16, 0.08, seed=11, fp32=True)
+    rng = np.random.default_rng(2)
+    a1 = rng.integers(1, 600, size=24)
+    a2 = np.array([rng.integers(0, a) for a in a1])
+    plist = np.unique(a1 * (a1 - 1) // 2 + a2).astype(np.int64)
+    fast = gc.kraskov_corrmatrix(x, 100, pair_list=plist)
+    exact = gc.kraskov_corrmatrix(x, 100, pair_list=plist, path=gc.PATH_EXACT_FP64)
+    np.testing.assert_array_equal(fast, exact)
+    assert np.count_nonzero(fast[np.tril_indices(600, -1)]) == len(plist)
+
+
 def test_shard_equals_full(gc, small_x):
     full = gc.kraskov_corrmatrix(small_x, 10)
     part = gc.kraskov_corrmatrix(small_x, 10, pairs=(100, 777))

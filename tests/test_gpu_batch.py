@@ -27,3 +27,18 @@ def test_batch_single_trajectory_and_errors(gc, small_x, golden):
     with pytest.raises(gc.GCError):
         gc.ksg_batch([small_x], [small_x.shape[1]])  # k must be below nframes
     gc.ksg_batch_release()
+
+
+def test_batch_several_waves(gc):
+    """A 420 x 4000 trajectory's sorted rows exceed the batch's row budget,
+    so its queries run in several waves beside a small trajectory; both
+    matrices equal the single-trajectory results."""
+    from gmx_correlation_b200.synth import synth_traj
+    xs = [synth_traj(420, 4000, 8, 0.08, 5, fp32=True), synth_traj(30, 600, 4, 0.06, 6, fp32=True)]
+    ks = [100, 10]
+    singles = [gc.kraskov_corrmatrix(x, k) for x, k in zip(xs, ks)]
+    mats = gc.ksg_batch(xs, ks)
+    for m, ref in zip(mats, singles):
+        np.testing.assert_array_equal(m, ref)
+    gc.ksg_batch_release()
+    gc.release_cache()

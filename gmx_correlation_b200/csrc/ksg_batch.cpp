@@ -7,10 +7,14 @@
 // the row sort, the walk and the finish whose tasks are drawn from every
 // trajectory still active (a global task counter over a prefix table of
 // per-trajectory descriptors), so trajectories of uneven atom and frame
-// counts and different k share the GPU.  The whole sequence (normalisation,
-// FP32 rows, waves, exact fix-up, MI reduction) is captured once into a CUDA
-// graph and replayed; the walk's launch shape (warps per CTA, atom-tile size
-// of the pair order) is chosen by timing the candidates on the first wave the
+// counts and different k share the GPU.  Trajectories are grouped by row
+// length (up to 2048, 4096, 8192 or more sorted entries per row), and each
+// group runs its own waves with the row-sort and walk shapes of its longest
+// rows, so short trajectories do not take the shapes long ones need.  The
+// whole sequence (normalisation, FP32 rows, every group's waves, exact
+// fix-up, MI reduction) is captured once into a CUDA graph and replayed; each
+// group's walk launch shape (atom-tile size of the pair order, query groups
+// per warp task) is chosen by timing the candidates on its first wave the
 // first time a shape class is seen.
 
 #include "gc_geom.h"
@@ -43,13 +47,29 @@ struct BatchTraj
     std::vector<double> host_mi;
 };
 
+// Trajectories of one row-length class and their launch tables.
+struct BatchGroup
+{
+    std::vector<size_t> members; // indices into BatchPlan::t
+    int                 maxT = 0, maxK = 0;
+    KsgLaunch           fl;
+    WalkConfig          cfg;
+};
+
+// Row-length class of a trajectory: its rows' sorted-entry count up to 2048,
+// 4096, 8192 or beyond (the row sort's and the walk's shapes change there).
+int row_class(int T)
+{
+    const int N = T - 1;
+    return N <= 2048 ? 0 : (N <= 4096 ? 1 : (N <= 8192 ? 2 : 3));
+}
+
 struct BatchPlan
 {
     int                                     device = 0, sms = 148;
     std::vector<std::unique_ptr<BatchTraj>> t;
     DevBuf<int>                             status;
-    KsgLaunch                               fl;
-    WalkConfig                              cfg;
+    std::vector<std::unique_ptr<BatchGroup>> groups;
     bool                                    tuned  = false;
     cudaStream_t                            stream = nullptr;
     cudaGraphExec_t                         exec   = nullptr;
@@ -73,10 +93,10 @@ BatchPlan*  g_batch[64] = {};
 // whose sorted rows fit the budget.  A trajectory split into several blocks
 // gets blocks of whole rounds of the walk CTA's warps (32 x warps queries),
 // so every warp has a query group in every round of a pair's task.
-std::vector<int> batch_blocks(const std::vector<std::unique_ptr<BatchTraj>>& t)
+std::vector<int> batch_blocks(const std::vector<const BatchTraj*>& t, double budget)
 {
     int maxT = 0;
-    for (const auto& b : t)
+    for (const auto* b : t)
         maxT = std::max(maxT, b->T);
     int warps  = 0;
     bool staged = false;
@@ -86,7 +106,7 @@ std::vector<int> batch_blocks(const std::vector<std::unique_ptr<BatchTraj>>& t)
     {
         std::vector<int> q;
         double           bytes = 0.0;
-        for (const auto& b : t)
+        for (const auto* b : t)
         {
             int Qb = ((b->T + waves - 1) / waves + 31) & ~31;
             if (Qb < b->T && Qb > quantum)
@@ -95,19 +115,19 @@ std::vector<int> batch_blocks(const std::vector<std::unique_ptr<BatchTraj>>& t)
             q.push_back(Qb);
             bytes += (double)b->natoms * (((b->T - 1) + 31) & ~31) * ((Qb + 31) & ~31) * 6.0;
         }
-        if (bytes <= kBatchBudget || waves >= maxT)
+        if (bytes <= budget || waves >= maxT)
             return q;
     }
 }
 
-gc_status build_launch(BatchPlan& bp, const WalkConfig& cfg)
+gc_status build_launch(BatchPlan& bp, BatchGroup& g, const WalkConfig& cfg)
 {
     int nw = 0;
-    for (const auto& b : bp.t)
-        nw = std::max(nw, b->ft.blocks());
+    for (size_t i : g.members)
+        nw = std::max(nw, bp.t[i]->ft.blocks());
     std::vector<std::vector<gc::WalkParams>> waves((size_t)nw);
     std::vector<gc::WalkParams>              traj;
-    for (size_t i = 0; i < bp.t.size(); ++i)
+    for (size_t i : g.members)
     {
         BatchTraj& b = *bp.t[i];
         GC_TRY(b.ft.set_pair_tile(cfg.pair_tile));
@@ -115,7 +135,8 @@ gc_status build_launch(BatchPlan& bp, const WalkConfig& cfg)
             waves[(size_t)w].push_back(b.ft.desc(b.X.p, b.cnt.p, bp.status.p + i, w));
         traj.push_back(b.ft.desc(b.X.p, b.cnt.p, bp.status.p + i, 0));
     }
-    return bp.fl.build(waves, traj, cfg);
+    g.cfg = cfg;
+    return g.fl.build(waves, traj, cfg);
 }
 
 // Everything after the input upload, in stream order (graph-capturable).
@@ -129,15 +150,17 @@ gc_status enqueue_all(BatchPlan& bp, cudaStream_t s)
         GC_TRY_CUDA(gc::launch_ksg_x32(b.X.p, b.natoms, b.T, b.ft.X32.p, b.ft.eps.p, s));
         GC_TRY(b.ft.clear(s));
     }
-    GC_TRY(bp.fl.enqueue(bp.sms, s));
+    for (auto& g : bp.groups)
+        GC_TRY(g->fl.enqueue(bp.sms, s));
     for (auto& b : bp.t)
         gc::launch_ksg_finalize(b->cnt.p, b->pairs, b->T, b->K, b->psi.p, b->mi.p, s);
     GC_TRY_CUDA(cudaGetLastError());
     return GC_OK;
 }
 
-// Times each candidate walk configuration on the first wave and keeps the
-// fastest (inputs must be uploaded; the status words are ignored here).
+// Times each candidate walk configuration on every group's first wave and
+// keeps the fastest per group (inputs must be uploaded; the status words are
+// ignored here).
 gc_status autotune(BatchPlan& bp)
 {
     cudaStream_t s = bp.stream;
@@ -147,51 +170,52 @@ gc_status autotune(BatchPlan& bp)
         gc::launch_ksg_prepare(b.xyz.p, b.natoms, b.T, b.X.p, bp.status.p + i, s);
         GC_TRY_CUDA(gc::launch_ksg_x32(b.X.p, b.natoms, b.T, b.ft.X32.p, b.ft.eps.p, s));
     }
-    int maxT = 0, maxK = 0;
-    for (const auto& b : bp.t)
-    {
-        maxT = std::max(maxT, b->T);
-        maxK = std::max(maxK, b->K);
-    }
     cudaEvent_t e0, e1;
     GC_TRY_CUDA(cudaEventCreate(&e0));
     GC_TRY_CUDA(cudaEventCreate(&e1));
-    float      best = 1e30f;
-    WalkConfig best_cfg;
-    gc_status  st = GC_OK;
-    for (const WalkConfig& c : walk_candidates(maxT))
+    gc_status st = GC_OK;
+    for (auto& gp : bp.groups)
     {
-        if ((st = build_launch(bp, c)) != GC_OK)
-            break;
-        float ms = 0.0f;
-        for (int rep = 0; rep < 2 && st == GC_OK; ++rep) // the first run warms up
+        BatchGroup& g    = *gp;
+        float      best = 1e30f;
+        WalkConfig best_cfg;
+        for (const WalkConfig& c : walk_candidates(g.maxT))
         {
-            for (auto& b : bp.t)
-                if ((st = b->ft.clear(s)) != GC_OK)
-                    break;
-            cudaEventRecord(e0, s);
-            if (st == GC_OK)
-                st = bp.fl.enqueue(bp.sms, s, 0, 0, false);
-            cudaEventRecord(e1, s);
-            if (cudaEventSynchronize(e1) != cudaSuccess)
-                st = fail(GC_ERR_CUDA, "autotune run failed");
-            cudaEventElapsedTime(&ms, e0, e1);
+            if ((st = build_launch(bp, g, c)) != GC_OK)
+                break;
+            float ms = 0.0f;
+            for (int rep = 0; rep < 2 && st == GC_OK; ++rep) // the first run warms up
+            {
+                for (size_t i : g.members)
+                    if ((st = bp.t[i]->ft.clear(s)) != GC_OK)
+                        break;
+                cudaEventRecord(e0, s);
+                if (st == GC_OK)
+                    st = g.fl.enqueue(bp.sms, s, 0, 0, false);
+                cudaEventRecord(e1, s);
+                if (cudaEventSynchronize(e1) != cudaSuccess)
+                    st = fail(GC_ERR_CUDA, "autotune run failed");
+                cudaEventElapsedTime(&ms, e0, e1);
+            }
+            if (st != GC_OK)
+                break;
+            if (ms < best)
+            {
+                best     = ms;
+                best_cfg = c;
+            }
         }
         if (st != GC_OK)
             break;
-        if (ms < best)
-        {
-            best     = ms;
-            best_cfg = c;
-        }
+        remember_walk_config(g.maxT, g.maxK, best_cfg);
+        if ((st = build_launch(bp, g, best_cfg)) != GC_OK)
+            break;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     GC_TRY(st);
-    remember_walk_config(maxT, maxK, best_cfg);
-    bp.cfg   = best_cfg;
     bp.tuned = true;
-    return build_launch(bp, best_cfg);
+    return GC_OK;
 }
 
 gc_status create_plan(const gc_traj_view* trajs, const int* ks, int ntraj, int device, std::unique_ptr<BatchPlan>& out)
@@ -221,14 +245,46 @@ gc_status create_plan(const gc_traj_view* trajs, const int* ks, int ntraj, int d
         bp->key.insert(bp->key.end(), {b->natoms, b->T, b->K});
         bp->t.push_back(std::move(b));
     }
-    const std::vector<int> q = batch_blocks(bp->t);
-    bp->cfg                  = walk_config(maxT, maxK);
+    (void)maxT;
+    (void)maxK;
+    // groups by row length; each gets a share of the row budget in
+    // proportion to the sorted rows of all its queries
+    int gid[4] = {-1, -1, -1, -1};
+    std::vector<double> group_bytes;
+    double              total_bytes = 0.0;
     for (size_t i = 0; i < bp->t.size(); ++i)
     {
-        BatchTraj& b = *bp->t[i];
-        GC_TRY(b.ft.create(b.natoms, b.T, b.K, 0, b.pairs, nullptr, nullptr, q[i], bp->cfg.pair_tile));
+        const BatchTraj& b = *bp->t[i];
+        const int        c = row_class(b.T);
+        if (gid[c] < 0)
+        {
+            gid[c] = (int)bp->groups.size();
+            bp->groups.push_back(std::make_unique<BatchGroup>());
+            group_bytes.push_back(0.0);
+        }
+        BatchGroup& g = *bp->groups[(size_t)gid[c]];
+        g.members.push_back(i);
+        g.maxT = std::max(g.maxT, b.T);
+        g.maxK = std::max(g.maxK, b.K);
+        const double all = (double)b.natoms * (((b.T - 1) + 31) & ~31) * ((b.T + 31) & ~31) * 6.0;
+        group_bytes[(size_t)gid[c]] += all;
+        total_bytes += all;
     }
-    GC_TRY(build_launch(*bp, bp->cfg));
+    for (size_t gi = 0; gi < bp->groups.size(); ++gi)
+    {
+        BatchGroup&                   g = *bp->groups[gi];
+        std::vector<const BatchTraj*> members;
+        for (size_t i : g.members)
+            members.push_back(bp->t[i].get());
+        const std::vector<int> q   = batch_blocks(members, kBatchBudget * group_bytes[gi] / total_bytes);
+        const WalkConfig       cfg = walk_config(g.maxT, g.maxK);
+        for (size_t m = 0; m < g.members.size(); ++m)
+        {
+            BatchTraj& b = *bp->t[g.members[m]];
+            GC_TRY(b.ft.create(b.natoms, b.T, b.K, 0, b.pairs, nullptr, nullptr, q[m], cfg.pair_tile));
+        }
+        GC_TRY(build_launch(*bp, g, cfg));
+    }
     out = std::move(bp);
     return GC_OK;
 }

@@ -225,7 +225,6 @@ gc_status create_plan(const gc_traj_view* trajs, const int* ks, int ntraj, int d
     GC_TRY_CUDA(cudaDeviceGetAttribute(&bp->sms, cudaDevAttrMultiProcessorCount, device));
     GC_TRY_CUDA(cudaStreamCreateWithFlags(&bp->stream, cudaStreamNonBlocking));
     GC_TRY(bp->status.alloc((size_t)ntraj));
-    int maxT = 0, maxK = 0;
     for (int i = 0; i < ntraj; ++i)
     {
         auto b    = std::make_unique<BatchTraj>();
@@ -233,8 +232,6 @@ gc_status create_plan(const gc_traj_view* trajs, const int* ks, int ntraj, int d
         b->T      = trajs[i].nframes;
         b->K      = ks[i];
         b->pairs  = (long)b->natoms * (b->natoms - 1) / 2;
-        maxT      = std::max(maxT, b->T);
-        maxK      = std::max(maxK, b->K);
         GC_TRY(b->xyz.alloc((size_t)b->natoms * b->T * 3));
         GC_TRY(b->X.alloc((size_t)b->natoms * b->T * 3));
         GC_TRY(b->psi.alloc((size_t)b->T + 1));
@@ -245,8 +242,6 @@ gc_status create_plan(const gc_traj_view* trajs, const int* ks, int ntraj, int d
         bp->key.insert(bp->key.end(), {b->natoms, b->T, b->K});
         bp->t.push_back(std::move(b));
     }
-    (void)maxT;
-    (void)maxK;
     // groups by row length; each gets a share of the row budget in
     // proportion to the sorted rows of all its queries
     int gid[4] = {-1, -1, -1, -1};

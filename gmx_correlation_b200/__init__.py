@@ -101,6 +101,8 @@ def lib() -> ctypes.CDLL:
         L.gc_last_error.restype = ctypes.c_char_p
         L.gc_opts_init.argtypes = [ctypes.POINTER(_Opts)]
         L.gc_ksg_matrix.argtypes = [ctypes.POINTER(_TrajView), ctypes.c_int, ctypes.POINTER(_Opts), dp]
+        L.gc_ksg_matrix_prepared.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.POINTER(_Opts), dp]
         L.gc_gauss_matrix.argtypes = [ctypes.POINTER(_TrajView), ctypes.POINTER(_Opts), dp]
         L.gc_gcmi_matrix.argtypes = [ctypes.POINTER(_TrajView), ctypes.POINTER(_Opts), dp]
         L.gc_te_matrix.argtypes = [ctypes.POINTER(_TrajView), ctypes.c_int, ctypes.c_int,
@@ -312,6 +314,20 @@ def kraskov_prepare(x, *, device: int = -1):
     v, o = _view(x), _opts(device)
     _check(lib().gc_ksg_prepare(ctypes.byref(v), ctypes.byref(o), _dptr(X), _dptr(psi), _dptr(scal)))
     return X, psi, scal
+
+
+def kraskov_corrmatrix_prepared(X, psi, k: int, *, path: int = PATH_AUTO, device: int = -1) -> np.ndarray:
+    """KSG MI matrix from rows kraskov_prepare normalised (X [3n, T], psi
+    [T+1]), as the reference's kraskov_corrmatrix_gpu(kr, natoms, mat, k)."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    psi = np.ascontiguousarray(psi, dtype=np.float64)
+    if X.ndim != 2 or X.shape[0] % 3 or psi.shape != (X.shape[1] + 1,):
+        raise ValueError("X must be [3*natoms, nframes] and psi [nframes + 1]")
+    n, T = X.shape[0] // 3, X.shape[1]
+    out = np.zeros(n * n)
+    o = _opts(device, path)
+    _check(lib().gc_ksg_matrix_prepared(_dptr(X), _dptr(psi), n, T, int(k), ctypes.byref(o), _dptr(out)))
+    return out.reshape(n, n)
 
 
 def kraskov_wrap(X, psi, a1: int, a2: int, k: int, *, device: int = -1) -> float:

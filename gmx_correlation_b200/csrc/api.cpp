@@ -146,6 +146,7 @@ struct gc_ksg_plan
     DevBuf<int2>     pair_ab; // explicit pair list as (a1, a2), empty for a range
     int              launches = 0;
     cudaEvent_t      ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t      ev_done = nullptr; // recorded after the last kernel of a run, on the run's stream
     // fast path workspace
     bool                  fast = false;
     gc::host::KsgTraj     ft;
@@ -250,6 +251,7 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
     GC_TRY_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
     GC_TRY_CUDA(cudaEventCreate(&p->ev0));
     GC_TRY_CUDA(cudaEventCreate(&p->ev1));
+    GC_TRY_CUDA(cudaEventCreateWithFlags(&p->ev_done, cudaEventDisableTiming));
     GC_TRY(p->X.alloc((size_t)3 * natoms * nframes));
     GC_TRY(p->psi.alloc((size_t)nframes + 1));
     GC_TRY(p->cnt.alloc((size_t)nframes * (size_t)(pc > 0 ? pc : 1)));
@@ -287,16 +289,21 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
     return GC_OK;
 }
 
-gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi, void* stream)
+} // extern "C"
+
+namespace {
+
+// One run of a plan: the normalisation of d_xyz into the plan's rows (or,
+// with d_xyz == nullptr, a finiteness check of rows the caller already
+// placed there), then the neighbour statistics and the MI reduction.
+gc_status plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi, cudaStream_t s)
 {
-    if (!p || !d_xyz || !d_pair_mi)
-        return fail(GC_ERR_INVALID, "null plan or device buffer");
-    DeviceScope dev(p->device);
-    GC_TRY(dev.st);
-    cudaStream_t s = stream ? (cudaStream_t)stream : p->stream;
-    p->launches    = 0;
+    p->launches = 0;
     GC_TRY_CUDA(cudaMemsetAsync(p->status.p, 0, sizeof(int), s));
-    gc::launch_ksg_prepare(d_xyz, p->natoms, p->T, p->X.p, p->status.p, s);
+    if (d_xyz)
+        gc::launch_ksg_prepare(d_xyz, p->natoms, p->T, p->X.p, p->status.p, s);
+    else
+        gc::launch_ksg_check_rows(p->X.p, (long)3 * p->natoms * p->T, p->status.p, s);
     ++p->launches;
     p->last_xyz    = d_xyz;
     p->last_mi     = d_pair_mi;
@@ -321,7 +328,21 @@ gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi
         p->launches += 1;
     }
     GC_TRY_CUDA(cudaGetLastError());
+    GC_TRY_CUDA(cudaEventRecord(p->ev_done, s));
     return GC_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+gc_status gc_ksg_plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi, void* stream)
+{
+    if (!p || !d_xyz || !d_pair_mi)
+        return fail(GC_ERR_INVALID, "null plan or device buffer");
+    DeviceScope dev(p->device);
+    GC_TRY(dev.st);
+    return plan_run(p, d_xyz, d_pair_mi, stream ? (cudaStream_t)stream : p->stream);
 }
 
 gc_status gc_ksg_plan_sync(gc_ksg_plan* p)
@@ -330,8 +351,9 @@ gc_status gc_ksg_plan_sync(gc_ksg_plan* p)
         return fail(GC_ERR_INVALID, "null plan");
     DeviceScope dev(p->device);
     GC_TRY(dev.st);
-    GC_TRY_CUDA(cudaStreamSynchronize(p->stream));
-    GC_TRY_CUDA(cudaDeviceSynchronize());
+    // The run may have been ordered on a caller's stream: wait for its last
+    // kernel only, not for the caller's other work on the device.
+    GC_TRY_CUDA(cudaEventSynchronize(p->ev_done));
     int st = 0;
     GC_TRY_CUDA(cudaMemcpy(&st, p->status.p, sizeof(int), cudaMemcpyDeviceToHost));
     p->handoffs = 0;
@@ -386,6 +408,14 @@ void gc_ksg_plan_destroy(gc_ksg_plan* p)
         return;
     {
         DeviceScope dev(p->device);
+        // The plan's pooled blocks go back to the device pool below, where the
+        // next plan may take them at once: the last run's kernels (on whatever
+        // stream it was ordered) must be done writing them first.
+        if (p->ev_done)
+        {
+            cudaEventSynchronize(p->ev_done);
+            cudaEventDestroy(p->ev_done);
+        }
         if (p->stream)
             cudaStreamDestroy(p->stream);
         if (p->ev0)
@@ -473,13 +503,19 @@ void gc_release_cache(void)
     gc::host::pool_release();
 }
 
-gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, double* mi)
+} // extern "C"
+
+namespace {
+
+// gc_ksg_matrix and gc_ksg_matrix_prepared: either trajectory coordinates
+// (traj) or already-normalised component rows X [3n][T] with their digamma
+// table psi [T+1].
+gc_status ksg_matrix_impl(const gc_traj_view* traj, const double* X, const double* psi_in, int n, int T, int k,
+                          const gc_opts* opts, double* mi)
 {
-    GC_TRY(check_view(traj));
     if (!mi)
         return fail(GC_ERR_INVALID, "null output matrix");
     const gc_opts o = opts ? *opts : defaults();
-    const int     n = traj->natoms, T = traj->nframes;
     long          pb = 0, pc = 0;
     GC_TRY(validate_ksg(n, T, k, o, &pb, &pc));
     DeviceScope dev(o.device);
@@ -493,19 +529,28 @@ gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, do
     key.path       = o.path;
     key.pair_begin = pb;
     key.pair_count = pc;
-    const bool   cacheable = o.pair_list == nullptr;
+    // A plan that holds a caller's digamma table is not kept for later calls.
+    const bool   cacheable = o.pair_list == nullptr && traj != nullptr;
     gc_ksg_plan* raw       = cacheable ? cache_take(cur, key) : nullptr;
     if (!raw)
         GC_TRY(gc_ksg_plan_create(n, T, k, &o, &raw));
     std::unique_ptr<gc_ksg_plan, void (*)(gc_ksg_plan*)> plan(raw, gc_ksg_plan_destroy);
-    if (!plan->io_xyz.p)
-    {
-        GC_TRY(plan->io_xyz.alloc((size_t)n * T * 3));
+    if (!plan->io_mi.p)
         GC_TRY(plan->io_mi.alloc((size_t)(pc > 0 ? pc : 1)));
-    }
     cudaStream_t s = plan->stream;
-    GC_TRY(upload_traj(traj, plan->io_xyz.p, s));
-    GC_TRY(gc_ksg_plan_run(plan.get(), plan->io_xyz.p, plan->io_mi.p, s));
+    if (traj)
+    {
+        if (!plan->io_xyz.p)
+            GC_TRY(plan->io_xyz.alloc((size_t)n * T * 3));
+        GC_TRY(upload_traj(traj, plan->io_xyz.p, s));
+        GC_TRY(plan_run(plan.get(), plan->io_xyz.p, plan->io_mi.p, s));
+    }
+    else
+    {
+        GC_TRY_CUDA(cudaMemcpyAsync(plan->X.p, X, sizeof(double) * 3 * (size_t)n * T, cudaMemcpyHostToDevice, s));
+        GC_TRY_CUDA(cudaMemcpyAsync(plan->psi.p, psi_in, sizeof(double) * ((size_t)T + 1), cudaMemcpyHostToDevice, s));
+        GC_TRY(plan_run(plan.get(), nullptr, plan->io_mi.p, s));
+    }
     GC_TRY(gc_ksg_plan_sync(plan.get()));
     std::vector<double> pm((size_t)pc);
     if (pc > 0)
@@ -539,6 +584,24 @@ gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, do
     if (cacheable)
         cache_put(cur, key, plan.release());
     return GC_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, double* mi)
+{
+    GC_TRY(check_view(traj));
+    return ksg_matrix_impl(traj, nullptr, nullptr, traj->natoms, traj->nframes, k, opts, mi);
+}
+
+gc_status gc_ksg_matrix_prepared(const double* X, const double* psi, int natoms, int nframes, int k,
+                                 const gc_opts* opts, double* mi)
+{
+    if (!X || !psi)
+        return fail(GC_ERR_INVALID, "null normalised rows or digamma table");
+    return ksg_matrix_impl(nullptr, X, psi, natoms, nframes, k, opts, mi);
 }
 
 gc_status gc_te_matrix(const gc_traj_view* traj, int k, int lag, const gc_opts* opts, double* te)

@@ -12,6 +12,7 @@
 
 #include "correlation_core.h"
 #include "gcmi.h"
+#include "kraskov_gpu.h"
 #include "transfer_entropy.h"
 #include "gmx_corr_b200.h"
 
@@ -73,6 +74,16 @@ void te_matrix(const t_traj* traj, double* mat, int k, int lag, bool /*use_gpu*/
 }
 
 bool gpu_available() { return gc_gpu_available() != 0; }
+bool kraskov_gpu_probe() { return gc_gpu_available() != 0; }
+
+void kraskov_corrmatrix_gpu(const t_kraskov* kr, int natoms, double* mat, int k)
+{
+    const int           N = kr->N;
+    std::vector<double> X((size_t)natoms * DIM * N);
+    for (int c = 0; c < natoms * DIM; ++c)
+        std::memcpy(X.data() + (size_t)c * N, kr->x[c], sizeof(double) * N);
+    check(gc_ksg_matrix_prepared(X.data(), kr->psi, natoms, N, k, nullptr, mat));
+}
 bool gcmi_gpu_available() { return gc_gpu_available() != 0; }
 bool te_gpu_available() { return gc_gpu_available() != 0; }
 

@@ -26,6 +26,8 @@ void set_last_error(const char* msg);
 // xyz [natoms][T][3] (mean-centred) -> X [3*natoms][T] normalised, min-shifted
 // (kraskov_prepare arithmetic), status bits on error.
 void launch_ksg_prepare(const double* xyz, int natoms, int T, double* X, int* status, cudaStream_t s);
+// Sets kStatNonFinite when any of the n doubles of already-normalised rows is not finite.
+void launch_ksg_check_rows(const double* X, long n, int* status, cudaStream_t s);
 
 // Exact FP64 brute-force KSG statistics for pairs [pair_begin, pair_begin+pair_count):
 // writes cnt[i * pair_count + pl] = n_x | n_y << 16 for every query frame i.

@@ -206,6 +206,24 @@ void launch_ksg_prepare(const double* xyz, int natoms, int T, double* X, int* st
     ksg_prepare_kernel<<<natoms, kPrepThreads, 0, s>>>(xyz, natoms, T, X, status);
 }
 
+// Rows handed in already normalised (kraskov_corrmatrix_gpu's t_kraskov):
+// flags a non-finite value, which is what a constant component becomes
+// after the reference's z-scoring (0 / 0).
+__global__ void ksg_check_rows_kernel(const double* __restrict__ X, long n, int* __restrict__ status)
+{
+    bool bad = false;
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+        bad |= !isfinite(X[e]);
+    if (__any_sync(kFull, bad) && (threadIdx.x & 31) == 0)
+        atomicOr(status, kStatNonFinite);
+}
+
+void launch_ksg_check_rows(const double* X, long n, int* status, cudaStream_t s)
+{
+    const long blocks = (n + 255) / 256;
+    ksg_check_rows_kernel<<<(unsigned)(blocks < 1184 ? (blocks > 0 ? blocks : 1) : 1184), 256, 0, s>>>(X, n, status);
+}
+
 void launch_ksg_exact(const double* X, int T, int K, long pair_begin, long pair_count, uint32_t* cnt,
                       cudaStream_t s, const int2* pair_ab)
 {

@@ -55,8 +55,9 @@ __device__ __forceinline__ double dist3d(const double* __restrict__ X64, int ato
     return fmax(fmax(fabs(r[i] - r[j]), fabs(r[T + i] - r[T + j])), fabs(r[2 * T + i] - r[2 * T + j]));
 }
 
-// One warp per atom: component midranges (X64 rows are min-shifted, so the
-// midrange is max/2), centred FP32 coordinates and the atom's error bound.
+// One warp per atom: component midranges c = (min + max) / 2 (for the
+// min-shifted rows kraskov_prepare makes, max / 2), centred FP32 coordinates
+// and the atom's error bound from the largest half-range R.
 __global__ void ksg_x32_kernel(const double* __restrict__ X64, int natoms, int T, float4* __restrict__ X32,
                                float* __restrict__ eps_atom)
 {
@@ -65,23 +66,25 @@ __global__ void ksg_x32_kernel(const double* __restrict__ X64, int natoms, int T
     if (a >= natoms)
         return;
     const double* r = X64 + (size_t)a * 3 * T;
-    double        mx[3];
+    double        c[3], R = 0.0;
     for (int d = 0; d < 3; ++d)
     {
-        double m = 0.0;
+        double lo = r[(size_t)d * T], hi = lo;
         for (int f = lane; f < T; f += 32)
-            m = fmax(m, r[(size_t)d * T + f]);
-        mx[d] = warp_max(m);
+        {
+            lo = fmin(lo, r[(size_t)d * T + f]);
+            hi = fmax(hi, r[(size_t)d * T + f]);
+        }
+        lo   = -warp_max(-lo);
+        hi   = warp_max(hi);
+        c[d] = 0.5 * (lo + hi);
+        R    = fmax(R, fmax(hi - c[d], c[d] - lo));
     }
-    const double c0 = 0.5 * mx[0], c1 = 0.5 * mx[1], c2 = 0.5 * mx[2];
     for (int f = lane; f < T; f += 32)
-        X32[(size_t)a * T + f] = make_float4((float)(r[f] - c0), (float)(r[T + f] - c1),
-                                             (float)(r[2 * T + f] - c2), 0.0f);
+        X32[(size_t)a * T + f] = make_float4((float)(r[f] - c[0]), (float)(r[T + f] - c[1]),
+                                             (float)(r[2 * T + f] - c[2]), 0.0f);
     if (lane == 0)
-    {
-        const double R = fmax(fmax(c0, c1), c2) * (1.0 + 0x1p-40);
-        eps_atom[a]    = __double2float_ru(R * 0x1p-21) + 1e-30f;
-    }
+        eps_atom[a] = __double2float_ru(R * (1.0 + 0x1p-40) * 0x1p-21) + 1e-30f;
 }
 
 // The descriptor owning task t: the largest d with prefix[d] <= t.

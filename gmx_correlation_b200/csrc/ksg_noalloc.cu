@@ -18,7 +18,11 @@
 // a host-side stand-in.  Its device address is looked up with
 // cudaGetSymbolAddress once per device (with that device current) on the
 // first call made on that device; that first call should therefore come
-// before any stream capture.
+// before any stream capture.  Under CUDA's lazy module loading that first
+// call is also what reserves the array on the device (it loads this file's
+// module), so it can fail for lack of memory where later calls cannot; an
+// application that hands all device memory to its own pool makes one
+// warm-up call first.  A cudaDeviceReset leaves the looked-up address stale.
 //
 // Every call shares the one array, which keeps the previous call's
 // contents; the status word is cleared on each call and every other region

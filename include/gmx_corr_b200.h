@@ -100,6 +100,18 @@ int gc_gpu_available(void);
  * the diagonal are written; the rest stays zero.  mi: natoms*natoms. */
 gc_status gc_ksg_matrix(const gc_traj_view* traj, int k, const gc_opts* opts, double* mi);
 
+/* The same KSG matrix from rows that kraskov_prepare already normalised:
+ * X [3*natoms][nframes] host doubles, component-major (comp = atom*3 + dim,
+ * the order of t_kraskov::x) and psi [nframes+1] the digamma table the
+ * neighbour counts index.  Replaces kraskov_corrmatrix_gpu
+ * (lib/kraskov_gpu.h:32, lib/kraskov_gpu.cu:225-308), which takes the
+ * prepared t_kraskov; unlike it there is no k <= 128 limit and exact ties
+ * follow mir_xnyn's scan order.  A non-finite row value (what a constant
+ * component becomes after z-scoring) gives GC_ERR_NONFINITE.  opts and mi
+ * as for gc_ksg_matrix. */
+gc_status gc_ksg_matrix_prepared(const double* X, const double* psi, int natoms, int nframes, int k,
+                                 const gc_opts* opts, double* mi);
+
 /* gc_ksg_matrix keeps the device workspace of its last call on each device
  * (a few GB at 247 atoms x 2000 frames) and reuses it when the next call has
  * the same shape (atoms, frames, k, path, pair range); explicit pair lists are
@@ -309,7 +321,13 @@ gc_status gc_ksg_screened(const gc_traj_view* traj, int k, gc_screen_model* mode
  * default stream).  Runs on the calling thread's current device and returns
  * after the work has finished (it synchronises the stream to check the
  * input-status word).  The first call on a device looks up the array's
- * device address, so it should come before any stream capture.  All calls
+ * device address, so it should come before any stream capture.  With CUDA's
+ * lazy module loading (the default) that first call is also what reserves
+ * the array on the device (CUDA_MODULE_LOADING=EAGER reserves it when the
+ * library loads), so a host application that gives all device memory to its
+ * own pool should make one warm-up call before doing so; later calls reserve
+ * nothing.  After a cudaDeviceReset the looked-up address is stale: do not
+ * call this entry point on that device again in the same process.  All calls
  * share the one array: calls whose work overlaps on the GPU race. */
 gc_status gc_ksg_pair_mi_noalloc(const double* d_xyz, int natoms, int nframes, int k, double* d_pair_mi, void* stream);
 

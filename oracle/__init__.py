@@ -21,7 +21,12 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "libgcoracle.so"
 REF_SO = HERE / "_ref" / "libgcref.so"
-REF_SRC = Path(os.environ.get("GMXCORR_REFERENCE", "/root/reference"))
+# The reference checkout: $GMXCORR_REFERENCE, else a `reference` directory
+# beside this repository's root.  Only build() reads it; the compiled
+# libraries under _ref/ are all the checkers need afterwards.
+_ROOT = HERE.parent
+REF_SRC = Path(os.environ["GMXCORR_REFERENCE"]) if os.environ.get("GMXCORR_REFERENCE") else (
+    _ROOT.parent / "reference")
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)

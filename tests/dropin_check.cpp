@@ -5,9 +5,11 @@
 // coords.bin: int32 natoms, int32 nframes, then natoms*nframes*3 doubles.
 #include "correlation_core.h"
 #include "gcmi.h"
+#include "kraskov_gpu.h"
 #include "transfer_entropy.h"
 
 #include <cstdio>
+#include <algorithm>
 #include <cstdlib>
 #include <stdexcept>
 #include <string>
@@ -58,6 +60,10 @@ int main(int argc, char** argv)
     kraskov_prepare(&traj, &kr);
     std::vector<double> w(1, kraskov_wrap(&kr, 1, 0, k));
     dump(pre + "wrap.bin", w);
+    // the legacy device-facing entry on the prepared workspace
+    std::fill(m.begin(), m.end(), -1.0);
+    kraskov_corrmatrix_gpu(&kr, n, m.data(), k);
+    dump(pre + "ksg_gpu.bin", m);
     kraskov_done(&kr);
     // input validation keeps the reference's exception and message
     t_traj one = traj;
@@ -72,6 +78,7 @@ int main(int argc, char** argv)
         std::printf("throw: %s\n", e.what());
     }
     std::printf("gpu_available=%d\n", gpu_available() ? 1 : 0);
+    std::printf("kraskov_gpu_probe=%d\n", kraskov_gpu_probe() ? 1 : 0);
     done_traj(&traj);
     return 0;
 }

@@ -58,3 +58,18 @@ def test_no_device_is_an_error_not_a_fallback(gc):
     with pytest.raises(gc.GCError) as e:
         gc.kraskov_corrmatrix(x, 4)
     assert e.value.status == 2
+
+
+def test_cpp_dropin_links_every_reference_symbol(gc, tmp_path):
+    """The reference front end's C++ calls (lib/correlation_core.h:65-88,
+    lib/gcmi.h:8-10, lib/transfer_entropy.h:8-10, lib/kraskov_gpu.h:20,32)
+    resolve against the library: tests/dropin_check.cpp, which calls every one
+    of them, links (nothing runs here)."""
+    import shutil
+    import subprocess
+    cxx = "/usr/bin/g++" if shutil.which("/usr/bin/g++") else "g++"
+    pkg = ROOT / "gmx_correlation_b200"
+    res = subprocess.run([cxx, "-O0", "-std=c++17", f"-I{pkg / 'csrc' / 'dropin'}",
+                          str(ROOT / "tests" / "dropin_check.cpp"), "-o", str(tmp_path / "dropin_check"),
+                          f"-L{pkg}", "-lgmxcorr_b200", "-Wl,--no-undefined"], capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr

@@ -32,8 +32,11 @@ def test_dropin_matches_oracle(dropin_bin, oracle, golden, small_x, tmp_path):
                          text=True, check=True)
     assert "throw: kraskov_corrmatrix: need at least 2 atoms" in res.stdout
     assert "gpu_available=1" in res.stdout
+    assert "kraskov_gpu_probe=1" in res.stdout
     load = lambda name: np.fromfile(tmp_path / name).reshape(n, n)  # noqa: E731
     np.testing.assert_array_equal(load("ksg.bin"), oracle.ksg_matrix(x, 10))
+    # legacy kraskov_corrmatrix_gpu on the prepared workspace: every entry written
+    np.testing.assert_array_equal(load("ksg_gpu.bin"), oracle.ksg_matrix(x, 10))
     np.testing.assert_allclose(load("gauss.bin"), oracle.gauss_matrix(x), rtol=1e-12, atol=1e-14)
     np.testing.assert_allclose(load("gcmi.bin"), oracle.gcmi_matrix(x), rtol=1e-12, atol=1e-14)
     np.testing.assert_array_equal(load("te.bin"), oracle.te_matrix(x, 10, 2))

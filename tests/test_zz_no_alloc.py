@@ -53,3 +53,35 @@ def test_noalloc_rejects_sizes_beyond_its_limit(gc):
     with pytest.raises(gc.GCError) as e:
         gc.ksg_pair_mi_noalloc(d.data_ptr(), 4, 1025, 5, out.data_ptr(), 0)
     assert e.value.status == 1
+
+
+def test_noalloc_call_reserves_no_device_memory(gc):
+    """After the first call (which, under lazy module loading, is what reserves
+    the fixed array), a call leaves the device's free memory unchanged."""
+    torch = pytest.importorskip("torch")
+    from gmx_correlation_b200.synth import synth_traj
+    x = synth_traj(24, 500, 4, 0.08, seed=43, fp32=True)
+    first = _call(gc, torch, x, 8)
+    d_xyz = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    d_out = torch.zeros(24 * 23 // 2, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    gc.ksg_pair_mi_noalloc(d_xyz.data_ptr(), 24, 500, 8, d_out.data_ptr(), 0)
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+    np.testing.assert_array_equal(d_out.cpu().numpy(), first)
+
+
+def test_noalloc_nonfinite_input_then_valid_call(gc):
+    """A NaN coordinate reports GC_ERR_NONFINITE through the shared status
+    word; the next valid call clears it and still equals gc_ksg_matrix."""
+    torch = pytest.importorskip("torch")
+    from gmx_correlation_b200.synth import synth_traj
+    x = synth_traj(9, 300, 4, 0.08, seed=44)
+    bad = x.copy()
+    bad[3, 17, 1] = np.nan
+    with pytest.raises(gc.GCError) as e:
+        _call(gc, torch, bad, 6)
+    assert e.value.status == 5
+    np.testing.assert_array_equal(_call(gc, torch, x, 6), _pairs_of(gc.kraskov_corrmatrix(x, 6)))

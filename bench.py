@@ -270,6 +270,78 @@ def screened_variant(gc, x, k, plain_e2e_s: float, device: int, reps: int = 3):
             "calibrated_1e-2": cal, "audit_only": loose}
 
 
+TE_OPS_PER_EVAL = 18  # 9 |d|, 8 max, 1 threshold compare per 9-D joint distance-eval
+
+
+def te_variant(gc, torch, x, k: int, lag: int, dev, local: int, mix_ops: float, reps: int = 3,
+               cpu: bool = True):
+    """Transfer entropy TE(a2 -> a1) of every ordered pair at the same
+    workload (lib/transfer_entropy.cpp:63-221), lag `lag`: the device-resident
+    TE plan timed with CUDA events (L2 flushed between runs), the end-to-end
+    gc_te_matrix call from pinned host memory, and the reference's own OpenMP
+    te_matrix on a 16-atom subset of the trajectory (240 ordered pairs)."""
+    n, T = x.shape[0], x.shape[1]
+    nv = T - lag
+    d_xyz = torch.from_numpy(x).to(dev)
+    d_te = torch.zeros((n, n), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    plan = gc.TePlan(n, T, k, lag, device=local)
+    stream = torch.cuda.current_stream(dev)
+    plan.run(d_xyz.data_ptr(), d_te.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    plan.sync()
+    step, kern = [], []
+    for _ in range(reps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.run(d_xyz.data_ptr(), d_te.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        step.append(e0.elapsed_time(e1))
+        kern.append(plan.kernel_ms)
+    plan.sync()
+    pairs = plan.pairs
+    ms, kms = statistics.mean(step), statistics.mean(kern)
+    evals = pairs * nv * (nv - 1)
+    out = {"metric": "TE ordered pairs/s", "value": pairs / (ms / 1e3), "unit": "pairs/s", "lag": lag, "k": k,
+           "ms_per_matrix": ms, "kernel_ms": kms, "ordered_pairs": pairs,
+           "path": "sorted-row walk + exact fp64 repair" if plan.is_walk else "fp32 brute force + fp64 repair",
+           "handed_to_exact": plan.handoffs, "walk_entries_per_query": round(plan.walk_mean, 1),
+           "gpu_launches": plan.launches,
+           "roofline": {"bound": "fp32", "achieved": evals * TE_OPS_PER_EVAL / (kms / 1e3) / 1e12,
+                        "peak": mix_ops / 1e12, "unit": "TOP/s",
+                        "frac": evals * TE_OPS_PER_EVAL / (kms / 1e3) / mix_ops,
+                        "distance_evals_per_s": evals / (kms / 1e3),
+                        "note": "reuse-normalised: T(T-1) 9-D evals per ordered pair x 18 ops over the "
+                                "neighbour kernels' time"}}
+    plan.close()
+    x_pinned = torch.from_numpy(x).pin_memory().numpy()
+    gc.te_matrix(x_pinned, k, lag, device=local)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        gc.te_matrix(x_pinned, k, lag, device=local)
+    e2e = (time.perf_counter() - t0) / reps
+    out["e2e"] = {"value": pairs / e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(x.nbytes),
+                  "d2h_bytes_per_step": int(n * n * 8)}
+    if cpu:
+        try:
+            from oracle import Reference
+            ref = Reference()
+            sub = np.ascontiguousarray(x[:16])
+            threads = os.cpu_count() or 1
+            t0 = time.perf_counter()
+            ref.te_matrix(sub, k, lag, nthreads=threads)
+            dt = time.perf_counter() - t0
+            out["cpu_baseline"] = {"value": 16 * 15 / dt, "unit": "pairs/s", "cores": threads, "kind": "reference",
+                                   "sample": f"te_matrix on atoms 0-15 of the workload (240 ordered pairs, "
+                                             f"{dt:.1f} s, OpenMP)"}
+        except Exception as e:  # noqa: BLE001
+            out["cpu_baseline"] = {"unavailable": str(e)}
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -383,6 +455,11 @@ def run_ours(args):
                                       f"FFMA {fma_flops / 1e12:.1f} TFLOP/s"},
             "clocks": clocks,
         }
+        if ws == 1 and not args.no_te:
+            try:
+                out["te"] = te_variant(gc, torch, x, k, 1, dev, local, mix_ops, cpu=not args.no_cpu_baseline)
+            except Exception as e:  # noqa: BLE001
+                out["te"] = {"unavailable": str(e)}
         if ws == 1 and not args.no_screen:
             try:
                 out["screened"] = screened_variant(gc, x_pinned, k, e2e_s, local)
@@ -411,6 +488,7 @@ def main(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-screen", action="store_true", help="skip the MLP-screened variant")
+    ap.add_argument("--no-te", action="store_true", help="skip the transfer-entropy object")
     ap.add_argument("--natoms", type=int, default=0, help="smaller atom count (profiling cases only)")
     ap.add_argument("--path", type=int, default=0, help="0 fast (default), 1 exact FP64")
     args = ap.parse_args(argv)

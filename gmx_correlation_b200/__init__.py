@@ -132,6 +132,18 @@ def lib() -> ctypes.CDLL:
         L.gc_probe_fp32.argtypes = [ctypes.c_int, dp, dp]
         L.gc_ksg_pair_mi_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_void_p, ctypes.c_void_p]
+        L.gc_te_plan_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(_Opts), ctypes.POINTER(ctypes.c_void_p)]
+        L.gc_te_plan_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.gc_te_plan_sync.argtypes = [ctypes.c_void_p]
+        for name, res in (("gc_te_plan_pairs", ctypes.c_long), ("gc_te_plan_launches", ctypes.c_int),
+                          ("gc_te_plan_is_walk", ctypes.c_int), ("gc_te_plan_handoffs", ctypes.c_long),
+                          ("gc_te_plan_walk_mean", ctypes.c_double), ("gc_te_plan_kernel_ms", ctypes.c_float)):
+            getattr(L, name).argtypes = [ctypes.c_void_p]
+            getattr(L, name).restype = res
+        L.gc_te_plan_counts.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ip, ip, ip]
+        L.gc_te_plan_destroy.argtypes = [ctypes.c_void_p]
+        L.gc_te_plan_destroy.restype = None
         L.gc_ksg_plan_destroy.argtypes = [ctypes.c_void_p]
         L.gc_ksg_plan_destroy.restype = None
         L.gc_release_cache.restype = None
@@ -378,6 +390,51 @@ def ksg_pair_mi_noalloc(d_xyz: int, natoms: int, nframes: int, k: int, d_pair_mi
     (natoms <= 64, nframes <= 1024); pointers are raw device addresses."""
     _check(lib().gc_ksg_pair_mi_noalloc(ctypes.c_void_p(d_xyz), int(natoms), int(nframes), int(k),
                                         ctypes.c_void_p(d_pair_mi), ctypes.c_void_p(stream or 0)))
+
+
+class TePlan:
+    """Device-resident transfer-entropy plan (one natoms x nframes, k, lag shape)."""
+
+    def __init__(self, natoms: int, nframes: int, k: int, lag: int = 1, *, device: int = -1,
+                 path: int = PATH_AUTO):
+        self._h = ctypes.c_void_p()
+        o = _opts(device, path)
+        _check(lib().gc_te_plan_create(natoms, nframes, k, lag, ctypes.byref(o), ctypes.byref(self._h)))
+        self.natoms, self.nframes, self.k, self.lag = natoms, nframes, k, lag
+
+    def run(self, d_xyz: int, d_te: int, stream: int | None = None) -> None:
+        """Enqueue one TE matrix (natoms x natoms doubles at d_te)."""
+        _check(lib().gc_te_plan_run(self._h, ctypes.c_void_p(d_xyz), ctypes.c_void_p(d_te),
+                                    ctypes.c_void_p(stream or 0)))
+
+    def sync(self) -> None:
+        _check(lib().gc_te_plan_sync(self._h))
+
+    def counts(self, a1: int, a2: int):
+        """(n_xp, n_xfxp, n_ypxp) per query of TE(a2 -> a1) from the last run."""
+        nv = self.nframes - self.lag
+        out = [np.zeros(nv, np.int32) for _ in range(3)]
+        ip = ctypes.POINTER(ctypes.c_int32)
+        _check(lib().gc_te_plan_counts(self._h, int(a1), int(a2), *[o.ctypes.data_as(ip) for o in out]))
+        return tuple(out)
+
+    pairs = property(lambda self: int(lib().gc_te_plan_pairs(self._h)))
+    launches = property(lambda self: int(lib().gc_te_plan_launches(self._h)))
+    is_walk = property(lambda self: bool(lib().gc_te_plan_is_walk(self._h)))
+    handoffs = property(lambda self: int(lib().gc_te_plan_handoffs(self._h)))
+    walk_mean = property(lambda self: float(lib().gc_te_plan_walk_mean(self._h)))
+    kernel_ms = property(lambda self: float(lib().gc_te_plan_kernel_ms(self._h)))
+
+    def close(self) -> None:
+        if self._h:
+            lib().gc_te_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class KsgPlan:

@@ -604,69 +604,6 @@ gc_status gc_ksg_matrix_prepared(const double* X, const double* psi, int natoms,
     return ksg_matrix_impl(nullptr, X, psi, natoms, nframes, k, opts, mi);
 }
 
-gc_status gc_te_matrix(const gc_traj_view* traj, int k, int lag, const gc_opts* opts, double* te)
-{
-    GC_TRY(check_view(traj));
-    if (!te)
-        return fail(GC_ERR_INVALID, "null output matrix");
-    const gc_opts o = opts ? *opts : defaults();
-    const int     n = traj->natoms, T = traj->nframes;
-    if (k < 1)
-        return fail(GC_ERR_INVALID, "te_matrix: k must be at least 1");
-    if (lag < 0)
-        return fail(GC_ERR_INVALID, "te_matrix: lag must be non-negative");
-    std::memset(te, 0, sizeof(double) * (size_t)n * n);
-    const int Nv = T - lag;
-    if (Nv <= k)
-    {
-        std::fprintf(stderr, "Warning: TE: N_valid=%d <= k=%d; skipping.\n", Nv, k);
-        return GC_OK;
-    }
-    if (T > 65535)
-        return fail(GC_ERR_INVALID, "te_matrix: this build supports at most 65535 frames");
-    if (n < 2)
-        return GC_OK;
-    DeviceScope dev(o.device);
-    GC_TRY(dev.st);
-    StreamScope ss;
-    GC_TRY(ss.init(o.stream));
-    const long        np = (long)n * (n - 1);
-    DevBuf<double>    d_xyz, d_XT, d_psi, d_te;
-    DevBuf<uint2>     d_cnt;
-    DevBuf<int>       d_st;
-    DevBuf<float4>    d_X32;
-    DevBuf<float>     d_eps;
-    GC_TRY(d_xyz.alloc((size_t)n * T * 3));
-    GC_TRY(d_XT.alloc((size_t)n * T * 3));
-    GC_TRY(d_psi.alloc((size_t)Nv + 1));
-    GC_TRY(d_te.alloc((size_t)n * n));
-    GC_TRY(d_cnt.alloc((size_t)Nv * np));
-    GC_TRY(d_st.alloc(1));
-    const std::vector<double> psi = digamma_table(Nv);
-    GC_TRY_CUDA(cudaMemcpyAsync(d_psi.p, psi.data(), sizeof(double) * psi.size(), cudaMemcpyHostToDevice, ss.s));
-    GC_TRY(upload_traj(traj, d_xyz.p, ss.s));
-    GC_TRY_CUDA(cudaMemsetAsync(d_st.p, 0, sizeof(int), ss.s));
-    GC_TRY_CUDA(cudaMemsetAsync(d_te.p, 0, sizeof(double) * (size_t)n * n, ss.s));
-    gc::launch_transpose_components(d_xyz.p, n, T, d_XT.p, d_st.p, ss.s);
-    if (o.path == GC_PATH_EXACT_FP64)
-        gc::launch_te_exact(d_XT.p, n, T, k, lag, d_cnt.p, ss.s);
-    else
-    {
-        GC_TRY(d_X32.alloc((size_t)n * T));
-        GC_TRY(d_eps.alloc((size_t)n));
-        gc::launch_te_x32(d_XT.p, n, T, d_X32.p, d_eps.p, ss.s);
-        gc::launch_te_fast(d_XT.p, d_X32.p, d_eps.p, n, T, k, lag, d_cnt.p, ss.s);
-    }
-    gc::launch_te_finalize(d_cnt.p, n, T, k, lag, d_psi.p, d_te.p, ss.s);
-    GC_TRY_CUDA(cudaGetLastError());
-    GC_TRY_CUDA(cudaStreamSynchronize(ss.s));
-    int st = 0;
-    GC_TRY_CUDA(cudaMemcpy(&st, d_st.p, sizeof(int), cudaMemcpyDeviceToHost));
-    GC_TRY(status_to_error(st & gc::kStatNonFinite));
-    GC_TRY_CUDA(cudaMemcpy(te, d_te.p, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToHost));
-    return GC_OK;
-}
-
 static gc_status gauss_like(const gc_traj_view* traj, const gc_opts* opts, double* mi, int mode)
 {
     GC_TRY(check_view(traj));

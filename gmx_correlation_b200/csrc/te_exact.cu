@@ -11,6 +11,7 @@
 
 #include "gc_common.cuh"
 #include "gc_internal.h"
+#include "te_exact_query.cuh"
 
 namespace gc {
 
@@ -49,53 +50,14 @@ __global__ void __launch_bounds__(kTeWarps * 32)
     const int a1 = (int)(q / (natoms - 1));
     const int rr = (int)(q - (long)a1 * (natoms - 1));
     const int a2 = rr < a1 ? rr : rr + 1;
-    const double* __restrict__ A0 = XT + (size_t)(a1 * 3 + 0) * T;
-    const double* __restrict__ A1 = XT + (size_t)(a1 * 3 + 1) * T;
-    const double* __restrict__ A2 = XT + (size_t)(a1 * 3 + 2) * T;
-    const double* __restrict__ B0 = XT + (size_t)(a2 * 3 + 0) * T;
-    const double* __restrict__ B1 = XT + (size_t)(a2 * 3 + 1) * T;
-    const double* __restrict__ B2 = XT + (size_t)(a2 * 3 + 2) * T;
     const int Nv = T - lag;
     const int i0 = qb * kTeQBlock, i1 = min(Nv, i0 + kTeQBlock);
-    unsigned* h  = hist[warp];
-
 #pragma unroll 1
     for (int qi = i0 + warp; qi < i1; qi += kTeWarps)
     {
-        const double f0 = A0[qi + lag], f1 = A1[qi + lag], f2 = A2[qi + lag];
-        const double p0 = A0[qi], p1 = A1[qi], p2 = A2[qi];
-        const double y0 = B0[qi], y1 = B1[qi], y2 = B2[qi];
-        auto sub = [&](int j, double& dfut, double& dpast, double& dy) {
-            dfut  = fmax(fmax(fabs(f0 - A0[j + lag]), fabs(f1 - A1[j + lag])), fabs(f2 - A2[j + lag]));
-            dpast = fmax(fmax(fabs(p0 - A0[j]), fabs(p1 - A1[j])), fabs(p2 - A2[j]));
-            dy    = fmax(fmax(fabs(y0 - B0[j]), fabs(y1 - B1[j])), fabs(y2 - B2[j]));
-        };
-        auto key = [&](int j, unsigned long long& k) -> bool {
-            if (j == qi)
-                return false;
-            double a, b, c;
-            sub(j, a, b, c);
-            k = dbits(fmax(fmax(a, b), c));
-            return true;
-        };
-        int          below;
-        const double eps = __longlong_as_double((long long)warp_select_u64(key, Nv, K, 56, h, lane, &below));
-        int nxfxp = 0, nypxp = 0, nxp = 0;
-        for (int j = lane; j < Nv; j += 32)
-        {
-            if (j == qi)
-                continue;
-            double a, b, c;
-            sub(j, a, b, c);
-            nxfxp += fmax(a, b) < eps;
-            nypxp += fmax(b, c) < eps;
-            nxp += b < eps;
-        }
-        nxfxp = __reduce_add_sync(kFull, nxfxp);
-        nypxp = __reduce_add_sync(kFull, nypxp);
-        nxp   = __reduce_add_sync(kFull, nxp);
+        const uint2 c = te_exact_query(XT, T, K, lag, a1, a2, qi, hist[warp], lane);
         if (lane == 0)
-            cnt[(size_t)qi * npairs + q] = make_uint2((unsigned)nxp | ((unsigned)nxfxp << 16), (unsigned)nypxp);
+            cnt[(size_t)qi * npairs + q] = c;
     }
 }
 

@@ -144,6 +144,42 @@ gc_status gc_gcmi_matrix(const gc_traj_view* traj, const gc_opts* opts, double* 
  * When nframes - lag <= k the matrix is all zeros, as in the reference. */
 gc_status gc_te_matrix(const gc_traj_view* traj, int k, int lag, const gc_opts* opts, double* te);
 
+/* ---- Device-resident transfer-entropy plan ------------------------------
+ * Owns every device workspace of one (natoms, nframes, k, lag) shape;
+ * gc_te_matrix runs one.  gc_te_plan_run reads device coordinates d_xyz
+ * ([natoms][nframes][3] doubles) and writes the whole TE matrix to device
+ * memory d_te (natoms*natoms, the conventions of gc_te_matrix), ordered on
+ * `stream` (NULL = the plan's stream); nothing is synchronised.  The
+ * default path sorts each atom's target-embedding and marginal distance
+ * rows and walks them with FP32 distances and an exact FP64 repair (rows of
+ * up to 16385 frames); GC_PATH_EXACT_FP64 and longer trajectories use the
+ * brute-force kernels.  Requires natoms >= 2 and nframes - lag > k.
+ * No counterpart type in the reference (te_matrix computes and returns). */
+typedef struct gc_te_plan gc_te_plan;
+
+gc_status gc_te_plan_create(int natoms, int nframes, int k, int lag, const gc_opts* opts, gc_te_plan** plan);
+gc_status gc_te_plan_run(gc_te_plan* plan, const double* d_xyz, double* d_te, void* stream);
+/* Waits for the last run; reports a non-finite coordinate. */
+gc_status gc_te_plan_sync(gc_te_plan* plan);
+/* Ordered pairs natoms * (natoms - 1). */
+long   gc_te_plan_pairs(const gc_te_plan* plan);
+int    gc_te_plan_launches(const gc_te_plan* plan);
+/* 1 when the plan runs the sorted-row walk. */
+int    gc_te_plan_is_walk(const gc_te_plan* plan);
+/* Queries of the last run handed to the exact FP64 kernel, and the mean
+ * number of sorted-row entries walked per (ordered pair, query) (valid
+ * after gc_te_plan_sync; 0 off the walk path). */
+long   gc_te_plan_handoffs(const gc_te_plan* plan);
+double gc_te_plan_walk_mean(const gc_te_plan* plan);
+/* Device time in milliseconds of the neighbour-statistics kernels of the
+ * last run (CUDA events on the run's stream). */
+float  gc_te_plan_kernel_ms(const gc_te_plan* plan);
+/* Per-query counts of the last run for TE(a2 -> a1), host arrays of
+ * nframes - lag entries (any may be NULL): the strict counts n_xp, n_xfxp
+ * and n_ypxp of lib/transfer_entropy.cpp:167-186. */
+gc_status gc_te_plan_counts(gc_te_plan* plan, int a1, int a2, int32_t* n_xp, int32_t* n_xfxp, int32_t* n_ypxp);
+void   gc_te_plan_destroy(gc_te_plan* plan);
+
 /* r = sqrt(1 - exp(-2/dim * MI)) for MI > 0, else 0; the 2000 diagonal
  * maps to 1.  Replaces pearsify (lib/correlation_core.cpp:461-469). */
 void gc_pearsify(double* mat, int n, int dim);

@@ -64,3 +64,46 @@ def test_te_fast_path_equals_exact(gc, n, T, k, lag, grid):
     fast = gc.te_matrix(x, k, lag)
     exact = gc.te_matrix(x, k, lag, path=gc.PATH_EXACT_FP64)
     np.testing.assert_array_equal(fast, exact)
+
+
+@pytest.mark.parametrize("n,T,k,lag,grid", [
+    (12, 900, 20, 1, 0.0),
+    (9, 1500, 100, 5, 0.0),
+    (8, 500, 10, 2, 0.02),    # exact distance ties at eps
+    (6, 3000, 100, 10, 0.0),  # rows of 2989 entries: the 512-thread row sort
+    (7, 700, 30, 0, 0.0),     # lag 0: future and past coincide
+    (10, 1200, 300, 1, 0.0),  # k >= 256: values below the bound counted apart
+    (5, 200, 190, 3, 0.0),    # k close to N_valid - 1
+])
+def test_te_walk_equals_exact(gc, n, T, k, lag, grid):
+    """The sorted-row TE walk gives the exact FP64 kernel's matrix bit for bit."""
+    from gmx_correlation_b200.synth import synth_traj
+    x = synth_traj(n, T, 4, 0.08, seed=7 * n + T + k + lag, fp32=not grid)
+    if grid:
+        x = np.round(x / grid) * grid
+    plan = gc.TePlan(n, T, k, lag)
+    assert plan.is_walk
+    plan.close()
+    np.testing.assert_array_equal(gc.te_matrix(x, k, lag), gc.te_matrix(x, k, lag, path=gc.PATH_EXACT_FP64))
+
+
+def test_te_walk_counts_equal_oracle(gc, oracle):
+    """Per-query counts n_xp, n_xfxp, n_ypxp of the walk against the oracle."""
+    torch = pytest.importorskip("torch")
+    from gmx_correlation_b200.synth import synth_traj
+    x = synth_traj(16, 1000, 6, 0.08, seed=77, fp32=True)
+    n, T, k, lag = 16, 1000, 50, 3
+    plan = gc.TePlan(n, T, k, lag)
+    d_xyz = torch.from_numpy(x).cuda()
+    d_te = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    plan.run(d_xyz.data_ptr(), d_te.data_ptr())
+    plan.sync()
+    assert plan.handoffs < 0.01 * plan.pairs * (T - lag)
+    for a1, a2 in [(0, 1), (5, 3), (15, 0), (7, 12)]:
+        d = oracle.te_pair(x, k, lag, a1, a2)
+        nxp, nxf, nyp = plan.counts(a1, a2)
+        np.testing.assert_array_equal(nxp, d["nxp"])
+        np.testing.assert_array_equal(nxf, d["nxfxp"])
+        np.testing.assert_array_equal(nyp, d["nypxp"])
+        assert d_te[a1, a2].item() == d["te"]
+    plan.close()

@@ -70,7 +70,8 @@ class _Opts(ctypes.Structure):
                 ("pair_end", ctypes.c_long), ("stream", ctypes.c_void_p),
                 ("detail_nx", ctypes.POINTER(ctypes.c_int32)),
                 ("detail_ny", ctypes.POINTER(ctypes.c_int32)),
-                ("pair_list", ctypes.POINTER(ctypes.c_int64)), ("pair_list_len", ctypes.c_long)]
+                ("pair_list", ctypes.POINTER(ctypes.c_int64)), ("pair_list_len", ctypes.c_long),
+                ("variant", ctypes.c_int)]
 
 
 class _ScreenOpts(ctypes.Structure):
@@ -199,10 +200,13 @@ def _view(x: np.ndarray) -> _TrajView:
     return v
 
 
-def _opts(device=-1, path=PATH_AUTO, pairs=None, stream=None, pair_list=None) -> _Opts:
+VARIANT_DEFAULT, VARIANT_HBM_GATHER = 0, 1
+
+
+def _opts(device=-1, path=PATH_AUTO, pairs=None, stream=None, pair_list=None, variant=VARIANT_DEFAULT) -> _Opts:
     o = _Opts()
     lib().gc_opts_init(ctypes.byref(o))
-    o.device, o.path = device, path
+    o.device, o.path, o.variant = device, path, variant
     if pairs is not None:
         o.pair_begin, o.pair_end = int(pairs[0]), int(pairs[1])
     if pair_list is not None:
@@ -441,9 +445,9 @@ class KsgPlan:
     """Device-resident KSG plan: inputs already in HBM, nothing allocated per run."""
 
     def __init__(self, natoms: int, nframes: int, k: int, *, device: int = -1, pairs=None,
-                 path: int = PATH_AUTO, pair_list=None):
+                 path: int = PATH_AUTO, pair_list=None, variant: int = VARIANT_DEFAULT):
         self._h = ctypes.c_void_p()
-        o = _opts(device, path, pairs, pair_list=pair_list)
+        o = _opts(device, path, pairs, pair_list=pair_list, variant=variant)
         _check(lib().gc_ksg_plan_create(natoms, nframes, k, ctypes.byref(o), ctypes.byref(self._h)))
         self.natoms, self.nframes, self.k = natoms, nframes, k
 

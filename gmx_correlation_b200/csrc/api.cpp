@@ -172,6 +172,8 @@ gc_status validate_ksg(int natoms, int T, int k, const gc_opts& o, long* pb, lon
         return fail(GC_ERR_INVALID, "kraskov_corrmatrix: k must be at least 1");
     if (T > 65535)
         return fail(GC_ERR_INVALID, "kraskov_corrmatrix: this build supports at most 65535 frames");
+    if (o.variant != GC_VARIANT_DEFAULT && o.variant != GC_VARIANT_HBM_GATHER)
+        return fail(GC_ERR_INVALID, "unknown gc_opts.variant");
     const long np = (long)natoms * (natoms - 1) / 2;
     if (o.pair_list)
     {
@@ -276,10 +278,21 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
     }
     if (p->fast)
     {
-        const gc::host::WalkConfig cfg = gc::host::walk_config(nframes, k);
+        gc::host::WalkConfig cfg = gc::host::walk_config(nframes, k);
+        const bool           hbm = o.variant == GC_VARIANT_HBM_GATHER;
+        if (hbm)
+        {
+            // the other marginal comes from unsorted distance rows in HBM: no
+            // staged coordinates, so the walk CTA takes the most warps
+            cfg.gather_u   = true;
+            cfg.staged     = false;
+            cfg.walk_warps = gc::kWalkWarps;
+        }
         GC_TRY(p->ft.create(natoms, nframes, k, pb, pc, o.pair_list, p->pair_ab.p,
-                            gc::host::ksg_block_queries(natoms, nframes, 16.0 * (1 << 30), 32 * cfg.walk_warps),
-                            cfg.pair_tile));
+                            gc::host::ksg_block_queries(natoms, nframes, 16.0 * (1 << 30), 32 * cfg.walk_warps,
+                                                        hbm ? 4.0 * ((nframes + 3) & ~3) / (((nframes - 1) + 31) & ~31)
+                                                            : 0.0),
+                            cfg.pair_tile, hbm));
         std::vector<std::vector<gc::WalkParams>> waves;
         for (int b = 0; b < p->ft.blocks(); ++b)
             waves.push_back({p->ft.desc(p->X.p, p->cnt.p, p->status.p, b)});
@@ -436,11 +449,11 @@ namespace {
 // are not cached.  gc_release_cache() frees the cached plans.
 struct PlanKey
 {
-    int  natoms = 0, nframes = 0, k = 0, path = 0;
+    int  natoms = 0, nframes = 0, k = 0, path = 0, variant = 0;
     long pair_begin = 0, pair_count = 0;
     bool operator==(const PlanKey& o) const
     {
-        return natoms == o.natoms && nframes == o.nframes && k == o.k && path == o.path &&
+        return natoms == o.natoms && nframes == o.nframes && k == o.k && path == o.path && variant == o.variant &&
                pair_begin == o.pair_begin && pair_count == o.pair_count;
     }
 };
@@ -527,6 +540,7 @@ gc_status ksg_matrix_impl(const gc_traj_view* traj, const double* X, const doubl
     key.nframes    = T;
     key.k          = k;
     key.path       = o.path;
+    key.variant    = o.variant;
     key.pair_begin = pb;
     key.pair_count = pc;
     // A plan that holds a caller's digamma table is not kept for later calls.

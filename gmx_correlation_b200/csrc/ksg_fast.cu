@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(THREADS) ksg_rows_kernel(WalkBatch B)
     __shared__ RowSortShared<THREADS> sh;
     sort_row<THREADS, R>(
         sh, T - 1, i, [&](int j) { return dist3f(q, xr[j]); }, w.S, w.P, ((size_t)a * (Lpad >> 2) * Qp + iq) * 4,
-        (size_t)Qp * 4);
+        (size_t)Qp * 4, w.U ? w.U + ((size_t)a * Qp + iq) * w.Tpad : nullptr);
 }
 
 namespace {
@@ -318,8 +318,10 @@ __device__ __forceinline__ unsigned long long pack_walk(int bstar, int prefix, i
 // the pair's coordinate rows are copied into shared memory per task.  LO
 // (every k of the launch below 256): entries below the lower bound L count
 // in histogram index 0 (at most k - 1 of them: they all have s < L, the k-th
-// walked-row value), so the per-entry update needs no separate test.
-template <bool STAGED, bool LO>
+// walked-row value), so the per-entry update needs no separate test.  GU:
+// the other marginal's distance d is read from its unsorted row in HBM
+// (WalkParams::U) instead of being recomputed from coordinates.
+template <bool STAGED, bool LO, bool GU>
 __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -371,8 +373,10 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
         const bool      live = g < ngroups && iq < p.Q;
         const int       iql  = live ? iq : 0;
         const LaneSetup u    = lane_setup(p, tk.a1, tk.a2, iql, p.i0 + iql, xa, xb);
-        // the other atom's coordinate row (shared memory when staged)
+        // the other atom's coordinate row (shared memory when staged), or
+        // its unsorted distance row of this query
         const float4* X32o = STAGED ? (u.wx ? sx + T : sx) : u.X32o;
+        const float*  Uo   = GU ? p.U + ((size_t)u.o * p.Qp + iql) * p.Tpad : nullptr;
         {
             uint4* h4 = reinterpret_cast<uint4*>(base);
             for (int e = lane; e < kWalkBuckets * 32 / 16; e += 32)
@@ -429,7 +433,7 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
             for (int q = 0; q < 4; ++q)
             {
                 tkn[q]          = sv[q] <= stop;
-                const float v   = fmaxf(sv[q], dist3f(u.xo, X32o[jv[q]]));
+                const float v   = fmaxf(sv[q], GU ? Uo[jv[q]] : dist3f(u.xo, X32o[jv[q]]));
                 bool        inc = tkn[q];
                 if (!LO)
                 {
@@ -1025,11 +1029,14 @@ void walk_shape(int maxT, int* warps, bool* staged)
     *warps      = w > 0 ? w : kWalkWarps;
 }
 
-cudaError_t launch_ksg_walk(const WalkBatch& b, int warps, bool staged, int sms, cudaStream_t s)
+cudaError_t launch_ksg_walk(const WalkBatch& b, int warps, bool staged, int sms, cudaStream_t s, bool gather_u)
 {
     const bool lo = b.maxK < 256;
-    void (*kernel)(WalkBatch) = staged ? (lo ? ksg_walk_kernel<true, true> : ksg_walk_kernel<true, false>)
-                                       : (lo ? ksg_walk_kernel<false, true> : ksg_walk_kernel<false, false>);
+    staged        = staged && !gather_u;
+    void (*kernel)(WalkBatch) =
+        gather_u ? (lo ? ksg_walk_kernel<false, true, true> : ksg_walk_kernel<false, false, true>)
+                 : (staged ? (lo ? ksg_walk_kernel<true, true, false> : ksg_walk_kernel<true, false, false>)
+                           : (lo ? ksg_walk_kernel<false, true, false> : ksg_walk_kernel<false, false, false>));
     const size_t smem = (staged ? (size_t)2 * b.maxT * 16 : 0) + (size_t)warps * kWalkBuckets * 32;
     cudaError_t  e    = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)

@@ -37,6 +37,11 @@ struct WalkParams
     int*                status;
     unsigned long long* walk_elems; // optional: total walked row entries
     unsigned*           reasons;    // optional [8]: hand-overs by cause
+    // optional unsorted distance rows of the block: the distance from query
+    // i0 + iq of atom a to frame j at U[((size_t)a * Qp + iq) * Tpad + j]
+    // (GC_VARIANT_HBM_GATHER: the walk reads the other marginal here)
+    float* U;
+    int    Tpad;
 };
 
 // One launch over the query blocks of several trajectories (or of one): the
@@ -74,7 +79,9 @@ int walk_max_staged_warps(int maxT);
 // Each launcher returns the launch status (cudaGetLastError right after it).
 cudaError_t launch_ksg_x32(const double* X64, int natoms, int T, float4* X32, float* eps_atom, cudaStream_t s);
 cudaError_t launch_ksg_rows(const WalkBatch& b, long long rows, cudaStream_t s);
-cudaError_t launch_ksg_walk(const WalkBatch& b, int warps, bool staged, int sms, cudaStream_t s);
+// gather_u: the other marginal's distances come from the descriptors' U rows.
+cudaError_t launch_ksg_walk(const WalkBatch& b, int warps, bool staged, int sms, cudaStream_t s,
+                            bool gather_u = false);
 cudaError_t launch_ksg_finish(const WalkBatch& b, int sms, cudaStream_t s);
 // Exact FP64 statistics for every queued hand-over of the batch's
 // descriptors, then for any hand-over mark a queue could not hold (a scan of

@@ -14,10 +14,10 @@
 namespace gc {
 namespace host {
 
-int ksg_block_queries(int natoms, int T, double budget, int quantum)
+int ksg_block_queries(int natoms, int T, double budget, int quantum, double extra_bytes_per_entry)
 {
     const int    Lpad = ((T - 1) + 31) & ~31;
-    const double row  = (double)natoms * Lpad * 6.0;
+    const double row  = (double)natoms * Lpad * (6.0 + extra_bytes_per_entry);
     long         q    = (long)(budget / row) / 32 * 32;
     q                 = q < 32 ? 32 : q;
     if (q >= T)
@@ -30,7 +30,7 @@ int ksg_block_queries(int natoms, int T, double budget, int quantum)
 }
 
 gc_status KsgTraj::create(int n, int nframes, int k, long pb, long pc, const int64_t* lst, const int2* d_ab, int q,
-                          int tile)
+                          int tile, bool unsorted_rows)
 {
     natoms     = n;
     T          = nframes;
@@ -49,6 +49,11 @@ gc_status KsgTraj::create(int n, int nframes, int k, long pb, long pc, const int
     GC_TRY(eps.alloc((size_t)natoms));
     GC_TRY(S.alloc((size_t)natoms * Qp * Lpad));
     GC_TRY(P.alloc((size_t)natoms * Qp * Lpad));
+    Tpad = (T + 3) & ~3;
+    if (unsorted_rows)
+        GC_TRY(U.alloc((size_t)natoms * Qp * Tpad));
+    else
+        U.reset();
     GC_TRY(wres.alloc((size_t)Q * (pc > 0 ? pc : 1)));
     // hand-over queue: ample for the rare hand-overs; overflow is caught by
     // the fix-up's scan of the counts
@@ -122,6 +127,8 @@ WalkParams KsgTraj::desc(const double* X, uint32_t* cnt, int* status, int b) con
     w.status     = status;
     w.walk_elems = walk_elems.p;
     w.reasons    = reasons.p;
+    w.U          = U.p;
+    w.Tpad       = Tpad;
     return w;
 }
 
@@ -209,7 +216,7 @@ gc_status KsgLaunch::enqueue(int sms, cudaStream_t s, int first_wave, int last_w
     for (int v = first_wave; v <= last_wave; ++v)
     {
         GC_TRY_CUDA(launch_ksg_rows(waves[(size_t)v], wave_rows[(size_t)v], s));
-        GC_TRY_CUDA(launch_ksg_walk(waves[(size_t)v], cfg.walk_warps, cfg.staged, sms, s));
+        GC_TRY_CUDA(launch_ksg_walk(waves[(size_t)v], cfg.walk_warps, cfg.staged, sms, s, cfg.gather_u));
         GC_TRY_CUDA(launch_ksg_finish(waves[(size_t)v], sms, s));
         launches += 3;
     }

@@ -19,6 +19,7 @@ struct WalkConfig
     bool staged     = false;
     int  pair_tile  = 16;
     int  chunk_mult = 4; // query groups per walk task = chunk_mult * walk_warps
+    bool gather_u   = false; // other marginal from precomputed HBM rows (GC_VARIANT_HBM_GATHER)
 };
 
 // Fast-path workspace of one trajectory (all pairs, a shard, or a list): the
@@ -39,10 +40,12 @@ struct KsgTraj
     PoolBuf<unsigned long long> wres, hq, walk_elems;
     PoolBuf<unsigned>           hq_len, reasons;
     PoolBuf<int>                pair_order;
+    PoolBuf<float>              U; // unsorted distance rows (GC_VARIANT_HBM_GATHER only)
+    int                         Tpad = 0;
 
     // Sizes the workspace for query blocks of Q frames (a multiple of 32, or T).
     gc_status create(int natoms, int T, int K, long pair_begin, long pair_count, const int64_t* list,
-                     const int2* d_pair_ab, int Q, int pair_tile);
+                     const int2* d_pair_ab, int Q, int pair_tile, bool unsorted_rows = false);
     // Reorders the pairs by atom tiles of the given side (device upload).
     gc_status set_pair_tile(int tile);
     int       blocks() const { return (T + Q - 1) / Q; }
@@ -55,7 +58,7 @@ struct KsgTraj
 // Query-block size for one trajectory whose sorted rows of a block must fit
 // in budget bytes; when the trajectory needs several blocks, a multiple of
 // quantum queries if the budget allows one.
-int ksg_block_queries(int natoms, int T, double budget, int quantum = 32);
+int ksg_block_queries(int natoms, int T, double budget, int quantum = 32, double extra_bytes_per_entry = 0.0);
 
 // Device tables of a sequence of waves: each wave one launch of the row
 // sort, the walk and the finish over the descriptors of that wave; then one

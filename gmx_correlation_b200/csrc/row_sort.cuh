@@ -30,7 +30,8 @@ __host__ __device__ constexpr int rows_skewed(int nbin) { return nbin + (nbin >>
 // for entry m (the transposed layout of the walk), the last 4-entry group
 // padded with NaN and frame 0.  Every thread of the CTA calls it; it uses
 // the dynamic shared memory (N2 * 8 + rows_skewed(nbin) * 8 bytes, N2 and
-// nbin as in row_sort_smem).
+// nbin as in row_sort_smem).  U_row (optional) receives the unsorted
+// distances at U_row[j].
 // Static shared memory of sort_row: the caller's kernel declares one (so a
 // kernel that sorts rows of several kinds holds it once).
 template <int THREADS>
@@ -45,7 +46,7 @@ struct RowSortShared
 template <int THREADS, int R, class DistFn>
 __device__ __forceinline__ void sort_row(RowSortShared<THREADS>& sh, int N, int i, DistFn&& dist,
                                          float* __restrict__ S, uint16_t* __restrict__ P, size_t base,
-                                         size_t gstride)
+                                         size_t gstride, float* __restrict__ U_row = nullptr)
 {
     extern __shared__ __align__(16) unsigned char rows_smem[];
     unsigned(&red_min)[THREADS / 32]       = sh.red_min;
@@ -95,6 +96,10 @@ __device__ __forceinline__ void sort_row(RowSortShared<THREADS>& sh, int N, int 
         }
     };
 
+    // optional unsorted copy of the row, indexed by frame (the query's own
+    // frame is left unwritten: no walk reads it)
+    if (U_row)
+        each([&](int, int m, float d) { U_row[frame_of(m)] = d; });
     unsigned kmin = 0xFFFFFFFFu, kmax = 0u;
     each([&](int, int, float d) {
         const unsigned k = __float_as_uint(d);

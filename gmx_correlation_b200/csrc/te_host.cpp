@@ -259,7 +259,9 @@ gc_status gc_te_plan_run(gc_te_plan* p, const double* d_xyz, double* d_te, void*
             GC_TRY_CUDA(gc::launch_te_rows(p->waves[w], p->wave_rows[w], s));
             GC_TRY_CUDA(gc::launch_te_walk(p->waves[w], p->warps, p->staged, p->sms, s));
             GC_TRY_CUDA(gc::launch_te_finish(p->waves[w], p->sms, s));
-            p->launches += 3;
+            GC_TRY_CUDA(cudaMemsetAsync(p->waves[w].counter, 0, sizeof(unsigned long long), s));
+            GC_TRY_CUDA(gc::launch_te_count(p->waves[w], p->warps, p->staged, p->sms, s));
+            p->launches += 4;
         }
         GC_TRY_CUDA(gc::launch_te_fixup(p->fix, p->sms, s));
         GC_TRY_CUDA(cudaEventRecord(p->ev1, s));

@@ -659,37 +659,15 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) te_finish_kernel(TeBatch
                     int n_xp = clo[2];
                     for (int pos = clo[2]; pos < clo[3]; ++pos)
                         n_xp += q64.past(M1.j(pos)) < eps;
-                    // n_ypxp: the shorter of the two M-row prefixes that can hold a
-                    // value below eps, the other marginal gathered
+                    // n_ypxp is counted by te_count_kernel over the shorter of
+                    // the two M-row prefixes that can hold a value below eps:
+                    // it gets eps (in wres) and the prefix (in cnt.y).
                     const int  end1 = clo[3], end2 = clo[4];
                     const bool on1  = end1 <= end2;
-                    const TeRow& er = on1 ? M1 : M2;
-                    const int    ne = on1 ? end1 : end2;
-                    const float  tlo_s = on1 ? tlo1 : tlo2;
-                    const float  tlo_o = on1 ? tlo2 : tlo1, thi_o = on1 ? thi2 : thi1;
-                    const float4* ox = on1 ? x2 : x1;
-                    const float4  oq = on1 ? qy : qp;
-                    int           n_ypxp = 0;
-                    for (int g0 = 0; g0 * 4 < ne; ++g0)
-                    {
-                        const float4 s4 = er.s4(g0);
-                        const uint2  j4 = er.j4(g0);
-#pragma unroll
-                        for (int q = 0; q < 4; ++q)
-                        {
-                            if (g0 * 4 + q < ne)
-                            {
-                                const int   j  = (int)u2at16(j4, q);
-                                const float sv = f4at(s4, q);
-                                const float ov = te3(oq, ox[j]);
-                                if (sv < tlo_s && ov < tlo_o)
-                                    ++n_ypxp;
-                                else if (ov <= thi_o)
-                                    n_ypxp += fmax(q64.past(j), q64.src(j)) < eps;
-                            }
-                        }
-                    }
-                    out = make_uint2((unsigned)n_xp | ((unsigned)n_xfxp << 16), (unsigned)n_ypxp);
+                    const int  ne   = on1 ? end1 : end2;
+                    p.wres[(size_t)pl * p.Q + iq] = (unsigned long long)__double_as_longlong(eps);
+                    out = make_uint2((unsigned)n_xp | ((unsigned)n_xfxp << 16),
+                                     (unsigned)ne | (on1 ? kTeCountOn1 : 0u));
                 }
             }
             if (reason)
@@ -708,6 +686,126 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) te_finish_kernel(TeBatch
             p.cnt[(size_t)pl * Nv + qi] = out;
         }
         __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// n_ypxp = #{j : max(D1(qi, j), Y(qi, j)) < eps}: one ordered pair per CTA
+// task with its two coordinate rows staged in shared memory (the walk's
+// task scheme), one query per lane.  Each lane enumerates the prefix the
+// finish kernel chose (the target's or the source's M row, every entry whose
+// FP32 value may lie below eps), gathers the other marginal from shared
+// memory, and re-evaluates in FP64 every entry within the error bound of
+// eps.
+// ---------------------------------------------------------------------------
+template <bool STAGED>
+__global__ void __launch_bounds__(1024, 1) te_count_kernel(TeBatch B)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ long long s_task;
+    __shared__ int       s_desc, s_next;
+    const int            lane = threadIdx.x & 31;
+    float4*              sx   = reinterpret_cast<float4*>(smem_raw);
+    const long long      total = B.wprefix[B.n];
+    TeTask               tk;
+    int                  dsc;
+    while (te_next_task(B, total, &s_task, &s_desc, &s_next, tk, dsc))
+    {
+        const TeParams& p       = B.d[dsc];
+        const int       T = p.T, Nv = p.Nv;
+        const int       ngroups = (p.Q + 31) >> 5;
+        const float4*   x1      = p.X32 + (size_t)tk.a1 * T;
+        const float4*   x2      = p.X32 + (size_t)tk.a2 * T;
+        if (STAGED)
+        {
+            for (int e = threadIdx.x; e < T; e += blockDim.x)
+            {
+                sx[e]     = x1[e];
+                sx[T + e] = x2[e];
+            }
+            __syncthreads();
+            x1 = sx;
+            x2 = sx + T;
+        }
+        const float e1 = p.eps_atom[tk.a1], e2a = p.eps_atom[tk.a2];
+        for (;;)
+        {
+            int gi = 0;
+            if (lane == 0)
+                gi = atomicAdd(&s_next, 1);
+            gi          = __shfl_sync(kFull, gi, 0);
+            const int g = tk.c * B.chunk + gi;
+            if (gi >= B.chunk || g >= ngroups)
+                break;
+            const int iq = g * 32 + lane;
+            if (iq < p.Q)
+            {
+                const int    qi = p.i0 + iq;
+                uint2* const cp = p.cnt + (size_t)tk.pl * Nv + qi;
+                const uint2  c  = *cp;
+                if (c.x != kTeHandOver)
+                {
+                    const double eps = __longlong_as_double((long long)p.wres[(size_t)tk.pl * p.Q + iq]);
+                    const int    ne  = (int)(c.y & 0xFFFFu);
+                    const bool   on1 = (c.y & kTeCountOn1) != 0u;
+                    const double es = on1 ? (double)e1 : (double)e2a, eo = on1 ? (double)e2a : (double)e1;
+                    const float  tlo_s = __double2float_rd(__dsub_rd(eps, es));
+                    const float  tlo_o = __double2float_rd(__dsub_rd(eps, eo));
+                    const float  thi_o = __double2float_ru(__dadd_ru(eps, eo));
+                    const TeRow  er = te_row(p.SM, p.PM, p, on1 ? tk.a1 : tk.a2, iq);
+                    const float4* ox = on1 ? x2 : x1;
+                    const float4  oq = ox[qi];
+                    const float4* Sg = reinterpret_cast<const float4*>(er.S);
+                    const uint2*  Pg = reinterpret_cast<const uint2*>(er.P);
+                    const size_t  gs = (size_t)p.Qp;
+                    const int     ng = (ne + 3) >> 2;
+                    int           n  = 0;
+                    float4        s4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                    uint2         j4 = make_uint2(0u, 0u);
+                    if (ng > 0)
+                    {
+                        s4 = Sg[0];
+                        j4 = Pg[0];
+                    }
+                    for (int g0 = 0; g0 < ng; ++g0)
+                    {
+                        // the next group is loaded while this one is counted
+                        const int    nx  = g0 + 1 < ng ? g0 + 1 : g0;
+                        const float4 ns4 = Sg[(size_t)nx * gs];
+                        const uint2  nj4 = Pg[(size_t)nx * gs];
+                        const float  sv[4] = {s4.x, s4.y, s4.z, s4.w};
+                        const unsigned jv[4] = {j4.x & 0xFFFFu, j4.x >> 16, j4.y & 0xFFFFu, j4.y >> 16};
+                        unsigned     amb = 0u;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                        {
+                            const bool  in = g0 * 4 + q < ne;
+                            const float ov = te3(oq, ox[jv[q]]);
+                            if (in && sv[q] < tlo_s && ov < tlo_o)
+                                ++n;
+                            else if (in && ov <= thi_o)
+                                amb |= 1u << q;
+                        }
+                        for (; amb; amb &= amb - 1) // rare: FP64 on the raw coordinates
+                        {
+                            const int     j  = (int)u2at16(j4, __ffs(amb) - 1);
+                            const double* ra = p.XT + (size_t)tk.a1 * 3 * T;
+                            const double* rb = p.XT + (size_t)tk.a2 * 3 * T;
+                            double        d  = 0.0;
+#pragma unroll 1
+                            for (int c3 = 0; c3 < 3; ++c3)
+                                d = fmax(d, fmax(fabs(ra[c3 * T + qi] - ra[c3 * T + j]),
+                                                 fabs(rb[c3 * T + qi] - rb[c3 * T + j])));
+                            n += d < eps;
+                        }
+                        s4 = ns4;
+                        j4 = nj4;
+                    }
+                    cp->y = (unsigned)n;
+                }
+            }
+        }
+        __syncthreads(); // every warp is done with the staged rows
     }
 }
 
@@ -861,6 +959,22 @@ cudaError_t launch_te_finish(const TeBatch& b, int sms, cudaStream_t s)
         return e;
     per_sm = per_sm < 1 ? 1 : per_sm;
     te_finish_kernel<<<sms * per_sm, kFinishWarps * 32, smem, s>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_te_count(const TeBatch& b, int warps, bool staged, int sms, cudaStream_t s)
+{
+    void (*kernel)(TeBatch) = staged ? te_count_kernel<true> : te_count_kernel<false>;
+    const size_t smem = staged ? (size_t)2 * b.maxT * 16 : 0;
+    cudaError_t  e    = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    int per_sm = 0;
+    e          = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, warps * 32, smem);
+    if (e != cudaSuccess)
+        return e;
+    per_sm = per_sm < 1 ? 1 : per_sm;
+    kernel<<<sms * per_sm, warps * 32, smem, s>>>(b);
     return cudaGetLastError();
 }
 

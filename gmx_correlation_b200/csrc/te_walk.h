@@ -47,6 +47,9 @@ struct TeParams
 };
 
 constexpr uint32_t kTeHandOver = 0xFFFFFFFFu;
+// Between te_finish_kernel and te_count_kernel cnt.y holds the prefix length
+// to enumerate for n_ypxp, with this bit set when it is the target's M row.
+constexpr uint32_t kTeCountOn1 = 1u << 16;
 
 // One launch over the query blocks of several trajectories (or of one), as
 // WalkBatch for the KSG kernels.  Every array lives in device memory.
@@ -67,6 +70,8 @@ struct TeBatch
 cudaError_t launch_te_rows(const TeBatch& b, long long rows, cudaStream_t s);
 cudaError_t launch_te_walk(const TeBatch& b, int warps, bool staged, int sms, cudaStream_t s);
 cudaError_t launch_te_finish(const TeBatch& b, int sms, cudaStream_t s);
+// n_ypxp of every (pair, query) the finish settled (its walk launch shape).
+cudaError_t launch_te_count(const TeBatch& b, int warps, bool staged, int sms, cudaStream_t s);
 // Exact FP64 statistics of every queued hand-over of the trajectories'
 // descriptors, then of any mark a full queue could not hold.
 cudaError_t launch_te_fixup(const TeBatch& b, int sms, cudaStream_t s);

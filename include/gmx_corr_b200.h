@@ -77,7 +77,16 @@ typedef struct gc_opts
      * detail arrays and plan outputs then follow the list order. */
     const int64_t* pair_list;
     long           pair_list_len;
+    /* GC_VARIANT_*: how the KSG fast path's walk obtains the distance of the
+     * marginal it does not walk (results are identical either way). */
+    int variant;
 } gc_opts;
+
+enum
+{
+    GC_VARIANT_DEFAULT    = 0, /* recomputed from the pair's coordinates staged in shared memory */
+    GC_VARIANT_HBM_GATHER = 1  /* read from per-(atom, query) distance rows precomputed in HBM */
+};
 
 /* Fills *o with the defaults (device -1, GC_PATH_AUTO, all pairs). */
 void gc_opts_init(gc_opts* o);

@@ -218,3 +218,24 @@ def test_k_equal_to_frames_minus_one(gc, oracle):
     x = synth_traj(4, 40, 3, 0.1, seed=9)
     np.testing.assert_array_equal(gc.kraskov_corrmatrix(x, 39), oracle.ksg_matrix(x, 39))
     np.testing.assert_array_equal(gc.kraskov_corrmatrix(x, 1), oracle.ksg_matrix(x, 1))
+
+
+@pytest.mark.parametrize("n,T,k", [(64, 500, 10), (20, 3000, 100), (10, 1200, 300)])
+def test_hbm_gather_variant_equals_default(gc, n, T, k):
+    """GC_VARIANT_HBM_GATHER (the walk reads the other marginal from unsorted
+    distance rows in HBM) gives the default walk's matrix bit for bit."""
+    torch = pytest.importorskip("torch")
+    from gmx_correlation_b200.synth import synth_traj
+    x = synth_traj(n, T, 6, 0.08, seed=n + 3 * T + k, fp32=True)
+    d_xyz = torch.from_numpy(x).cuda()
+    outs = []
+    for variant in (gc.VARIANT_DEFAULT, gc.VARIANT_HBM_GATHER):
+        plan = gc.KsgPlan(n, T, k, variant=variant)
+        out = torch.zeros(plan.pairs, dtype=torch.float64, device="cuda")
+        plan.run(d_xyz.data_ptr(), out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        plan.sync()
+        assert plan.is_fast
+        outs.append(out.cpu().numpy())
+        plan.close()
+    np.testing.assert_array_equal(outs[0], outs[1])

@@ -11,8 +11,10 @@ in HBM; the L2 is flushed (a 256 MiB write) between timed steps.  `value` is
 whole-job pairs/s; `e2e` is the same metric through the public C-ABI call
 gc_ksg_matrix from pinned host memory (H2D of the coordinates and D2H of the
 pair MI inside the timed region).  With N > 1 (torchrun, one rank per GPU)
-every rank processes its own independent trajectory (weak scaling, no
-data-path collective); timing is max over ranks.
+the same matrix is split into contiguous pair shards, one per rank (the
+reference's MPI split, lib/correlation_core.cpp:399-409), and one NCCL
+all-gather of the packed pair MI (8 bytes per pair) gives every rank the
+whole matrix inside the timed step (strong scaling); timing is max over ranks.
 
 The cpu_baseline object also carries `legacy_gpu`: the reference's own
 legacy CUDA KSG kernel (lib/kraskov_gpu.cu, built for sm_100a into
@@ -322,6 +324,39 @@ def large_variant(gc, torch, dev, local: int, mix_ops: float):
     return out
 
 
+def batch_variant(gc, local: int):
+    """The batched uneven workload (synth.batch_specs: 16 trajectories, 50-400
+    atoms, 500-4000 frames, k in {10, 50, 100}) through the batched entry
+    points, host arrays in and out: KSG MI, GCMI and TE at lags 1 / 5 / 10.
+    The first call of each (autotuning, graph capture) is untimed; the timed
+    second call replays the captured graphs."""
+    from gmx_correlation_b200.synth import batch_specs, batch_traj
+    specs = batch_specs()
+    xs = [batch_traj(sp) for sp in specs]
+    ks = [sp["k"] for sp in specs]
+    pairs = sum(x.shape[0] * (x.shape[0] - 1) // 2 for x in xs)
+    out = {"workload": "16 trajectories, atoms U[50,400], frames U[500,4000], k in {10,50,100}",
+           "trajectories": len(xs), "pairs": pairs, "ordered_pairs": 2 * pairs,
+           "timing": "host time of the second call (the first tunes and captures the graph)"}
+
+    def timed(fn):
+        fn()
+        t0 = time.perf_counter()
+        fn()
+        return time.perf_counter() - t0
+
+    dt = timed(lambda: gc.ksg_batch(xs, ks, device=local))
+    out["ksg"] = {"value": pairs / dt, "unit": UNIT, "seconds": dt}
+    dt = timed(lambda: gc.gcmi_batch(xs, device=local))
+    out["gcmi"] = {"value": pairs / dt, "unit": UNIT, "seconds": dt}
+    gc.batch_release()
+    for lag in (1, 5, 10):
+        dt = timed(lambda: gc.te_batch(xs, ks, lag, device=local))
+        out[f"te_lag{lag}"] = {"value": 2 * pairs / dt, "unit": "ordered pairs/s", "seconds": dt}
+    gc.batch_release()
+    return out
+
+
 TE_OPS_PER_EVAL = 18  # 9 |d|, 8 max, 1 threshold compare per 9-D joint distance-eval
 
 
@@ -413,19 +448,26 @@ def run_ours(args):
         torch.cuda.set_device(local)
     c = CONFIGS["ref"]
     natoms = args.natoms or c["natoms"]
-    x = synth_traj(natoms, c["nframes"], c["n_modes"], c["sigma_l"], seed=c["seed"] + rank, fp32=c["fp32"])
+    from gmx_correlation_b200.shard import gather_pairs, pair_shard, sharded_ksg_matrix
+    x = synth_traj(natoms, c["nframes"], c["n_modes"], c["sigma_l"], seed=c["seed"], fp32=c["fp32"])
     n, T, k = x.shape[0], x.shape[1], c["k"]
     npairs = n * (n - 1) // 2
+    pb, pe = pair_shard(npairs, rank, ws)
     dev = torch.device("cuda", local)
     d_xyz = torch.from_numpy(x).to(dev)
-    d_out = torch.empty(npairs, dtype=torch.float64, device=dev)
+    d_out = torch.empty(max(pe - pb, 1), dtype=torch.float64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    plan = gc.KsgPlan(n, T, k, device=local, path=args.path)
+    plan = gc.KsgPlan(n, T, k, device=local, path=args.path, pairs=(pb, pe) if ws > 1 else None)
     stream = torch.cuda.Stream(dev)  # a real stream handle (the legacy default stream is 0)
     torch.cuda.set_stream(stream)
 
-    for _ in range(args.warmup):
+    def step():
         plan.run(d_xyz.data_ptr(), d_out.data_ptr(), stream.cuda_stream)
+        if pg:  # every rank gets the whole packed pair list
+            gather_pairs(d_out[: pe - pb], npairs, pg)
+
+    for _ in range(args.warmup):
+        step()
         torch.cuda.synchronize(dev)
         plan.sync()
 
@@ -442,7 +484,7 @@ def run_ours(args):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        plan.run(d_xyz.data_ptr(), d_out.data_ptr(), stream.cuda_stream)
+        step()
         e1.record(stream)
         torch.cuda.synchronize(dev)
         step_ms.append(e0.elapsed_time(e1))
@@ -462,17 +504,25 @@ def run_ours(args):
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
-    value = ws * npairs / (ms_per_step / 1e3)
+    value = npairs / (ms_per_step / 1e3)  # one whole matrix per step, over all ranks
 
-    # end to end through the public C-ABI call, pinned host input
+    # end to end through the public C-ABI call, pinned host input (with N > 1
+    # each rank's shard, then the all-gather of the packed pair values)
     x_pinned = torch.from_numpy(x).pin_memory().numpy()
-    gc.kraskov_corrmatrix(x_pinned, k, device=local)
-    e2e_steps = max(1, min(args.steps, 3))
+
+    def e2e_call():
+        if pg:
+            sharded_ksg_matrix(x_pinned, k, pg)
+        else:
+            gc.kraskov_corrmatrix(x_pinned, k, device=local)
+
+    e2e_call()
+    e2e_steps = max(1, args.steps)
     if pg:
         pg.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        gc.kraskov_corrmatrix(x_pinned, k, device=local)
+        e2e_call()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     if pg:
         t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
@@ -483,20 +533,22 @@ def run_ours(args):
         mix_ops, fma_flops = gc.probe_fp32(local)
         kms = statistics.mean(kern_ms)
         kname = "ksg_neighbour_kernels" if plan.is_fast else "ksg_exact_kernel"
-        evals = npairs * T * (T - 1)
+        evals = (pe - pb) * T * (T - 1)  # this rank's shard
         achieved = evals * FP32_OPS_PER_EVAL / (kms / 1e3)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "strong" if ws > 1 else "weak",
             "vs_baseline": value / PUBLISHED_PAIRS_PER_S if natoms == c["natoms"] else None,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD if natoms == c["natoms"] else WORKLOAD.replace("247", str(natoms)),
-                       "variant": "plain", "pairs_per_gpu": npairs,
+                       "variant": "plain", "pairs_per_gpu": pe - pb,
+                       "parallelism": f"pair shards over {ws} GPUs + NCCL all-gather" if ws > 1 else "one GPU",
                        "l2": "256 MiB flush between timed steps",
                        "path": "fp32 sorted-row walk + exact fp64 repair" if plan.is_fast else "exact-fp64 brute force",
-                       "handed_to_exact": handoffs, "queries": npairs * T,
+                       "handed_to_exact": handoffs, "queries": (pe - pb) * T,
                        "walk_entries_per_query": round(walk_mean, 1), "handoff_reasons": reasons},
-            "e2e": {"value": ws * npairs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(x.nbytes),
+            "e2e": {"value": npairs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(x.nbytes),
                     "d2h_bytes_per_step": int(npairs * 8)},
             "gpu_launches": launches,
             "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": mix_ops / 1e12, "unit": "TOP/s",
@@ -507,6 +559,11 @@ def run_ours(args):
                                       f"FFMA {fma_flops / 1e12:.1f} TFLOP/s"},
             "clocks": clocks,
         }
+        if ws == 1 and not args.no_batch:
+            try:
+                out["batch"] = batch_variant(gc, local)
+            except Exception as e:  # noqa: BLE001
+                out["batch"] = {"unavailable": str(e)}
         if ws == 1 and not args.no_large:
             try:
                 out["large"] = large_variant(gc, torch, dev, local, mix_ops)
@@ -547,6 +604,7 @@ def main(argv=None):
     ap.add_argument("--no-screen", action="store_true", help="skip the MLP-screened variant")
     ap.add_argument("--no-te", action="store_true", help="skip the transfer-entropy object")
     ap.add_argument("--no-large", action="store_true", help="skip the 1000 x 5000 configuration")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven workload")
     ap.add_argument("--natoms", type=int, default=0, help="smaller atom count (profiling cases only)")
     ap.add_argument("--path", type=int, default=0, help="0 fast (default), 1 exact FP64")
     args = ap.parse_args(argv)

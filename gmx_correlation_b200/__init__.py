@@ -151,6 +151,12 @@ def lib() -> ctypes.CDLL:
         L.gc_ksg_batch.argtypes = [ctypes.POINTER(_TrajView), ctypes.POINTER(ctypes.c_int), ctypes.c_int,
                                    ctypes.POINTER(_Opts), ctypes.POINTER(dp)]
         L.gc_ksg_batch_release.restype = None
+        L.gc_te_batch.argtypes = [ctypes.POINTER(_TrajView), ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+                                  ctypes.POINTER(_Opts), ctypes.POINTER(dp)]
+        L.gc_te_batch_release.restype = None
+        L.gc_gcmi_batch.argtypes = [ctypes.POINTER(_TrajView), ctypes.c_int, ctypes.POINTER(_Opts),
+                                    ctypes.POINTER(dp)]
+        L.gc_gcmi_batch_release.restype = None
         fp = ctypes.POINTER(ctypes.c_float)
         L.gc_screen_features.argtypes = [ctypes.POINTER(_TrajView), ctypes.c_int, ctypes.POINTER(_Opts), fp, fp, fp]
         L.gc_screen_model_create.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
@@ -280,6 +286,57 @@ def ksg_batch(trajs, ks, *, device: int = -1):
     o = _opts(device)
     _check(lib().gc_ksg_batch(views, karr, len(xs), ctypes.byref(o), ptrs))
     return outs
+
+
+def _views(xs):
+    views = (_TrajView * len(xs))()
+    for v, x in zip(views, xs):
+        v.natoms, v.nframes = x.shape[0], x.shape[1]
+        v.xyz = _dptr(x)
+        v.rows = None
+    return views
+
+
+def te_batch(trajs, ks, lag: int = 1, *, device: int = -1):
+    """TE matrices (te[a1, a2] = TE(a2 -> a1)) of several trajectories at one
+    lag in one batched GPU run; ``ks`` one k per trajectory (or one int)."""
+    xs = [_coords(x) for x in trajs]
+    if isinstance(ks, int):
+        ks = [ks] * len(xs)
+    if len(ks) != len(xs):
+        raise ValueError("one k per trajectory")
+    outs = [np.zeros((x.shape[0], x.shape[0])) for x in xs]
+    ptrs = (ctypes.POINTER(ctypes.c_double) * len(xs))(*[_dptr(m) for m in outs])
+    karr = (ctypes.c_int * len(xs))(*[int(k) for k in ks])
+    o = _opts(device)
+    _check(lib().gc_te_batch(_views(xs), karr, len(xs), int(lag), ctypes.byref(o), ptrs))
+    return outs
+
+
+def gcmi_batch(trajs, *, device: int = -1):
+    """GCMI matrices of several trajectories in one batched GPU run."""
+    xs = [_coords(x) for x in trajs]
+    outs = [np.zeros((x.shape[0], x.shape[0])) for x in xs]
+    ptrs = (ctypes.POINTER(ctypes.c_double) * len(xs))(*[_dptr(m) for m in outs])
+    o = _opts(device)
+    _check(lib().gc_gcmi_batch(_views(xs), len(xs), ctypes.byref(o), ptrs))
+    return outs
+
+
+def corr_batch(trajs, ks, lags=(1, 5, 10), *, device: int = -1):
+    """Every matrix of the batched workload: KSG MI, GCMI and TE at each lag.
+    Returns {"ksg": [...], "gcmi": [...], "te": {lag: [...]}}."""
+    out = {"ksg": ksg_batch(trajs, ks, device=device), "gcmi": gcmi_batch(trajs, device=device), "te": {}}
+    for lag in lags:
+        out["te"][int(lag)] = te_batch(trajs, ks, lag, device=device)
+    return out
+
+
+def batch_release() -> None:
+    """Free the workspaces and graphs every batched entry point keeps."""
+    lib().gc_ksg_batch_release()
+    lib().gc_te_batch_release()
+    lib().gc_gcmi_batch_release()
 
 
 def ksg_batch_release() -> None:

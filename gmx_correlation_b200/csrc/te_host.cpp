@@ -11,6 +11,7 @@
 #include "host_common.h"
 #include "ksg_fast.h"
 #include "ksg_host.h"
+#include "te_host.h"
 #include "te_walk.h"
 
 #include <cuda_runtime.h>
@@ -23,38 +24,6 @@
 #include <vector>
 
 using namespace gc::host;
-
-struct gc_te_plan
-{
-    int          device = 0, sms = 148;
-    int          natoms = 0, T = 0, K = 0, lag = 0, Nv = 0, path = GC_PATH_AUTO;
-    long         npairs = 0; // ordered pairs
-    bool         walk   = false;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t  ev0 = nullptr, ev1 = nullptr, ev_done = nullptr;
-    PoolBuf<double> XT, psi;
-    PoolBuf<float4> X32;
-    PoolBuf<float>  eps;
-    PoolBuf<uint2>  cnt;
-    DevBuf<int>     status;
-    int             launches = 0;
-    // walk path
-    int                         Q = 0, Qp = 0, Lpad = 0, warps = 0;
-    bool                        staged = false;
-    PoolBuf<float>              SG, SM;
-    PoolBuf<uint16_t>           PG, PM;
-    PoolBuf<unsigned long long> wres, hq, walk_elems;
-    PoolBuf<unsigned>           hq_len, reasons;
-    PoolBuf<int>                pair_order;
-    DevBuf<gc::TeParams>        descs;
-    DevBuf<long long>           prefix;
-    DevBuf<unsigned long long>  counters;
-    std::vector<gc::TeBatch>    waves;
-    std::vector<long long>      wave_rows;
-    gc::TeBatch                 fix{};
-    long                        handoffs = 0;
-    double                      walk_mean = 0.0;
-};
 
 namespace {
 
@@ -91,104 +60,211 @@ std::vector<int> te_tile_order(int n)
     return order;
 }
 
-gc_status te_build_walk(gc_te_plan* p)
-{
-    const int n = p->natoms, Nv = p->Nv;
-    gc::walk_shape(p->T, &p->warps, &p->staged);
-    const int chunk = p->warps * 4;
-    // Sorted rows of one query block: G and M rows of every atom, within 16 GiB.
-    p->Q    = ksg_block_queries(2 * n, Nv, 16.0 * (1 << 30), 32 * p->warps);
-    p->Qp   = (p->Q + 31) & ~31;
-    p->Lpad = ((Nv - 1) + 31) & ~31;
-    const size_t rows = (size_t)n * p->Qp * p->Lpad;
-    GC_TRY(p->SG.alloc(rows));
-    GC_TRY(p->SM.alloc(rows));
-    GC_TRY(p->PG.alloc(rows));
-    GC_TRY(p->PM.alloc(rows));
-    GC_TRY(p->wres.alloc((size_t)p->Q * p->npairs));
-    const double hq_want = 0.01 * (double)p->npairs * Nv + 4096.0;
-    const unsigned hq_cap = (unsigned)(hq_want < 16777216.0 ? hq_want : 16777216.0);
-    GC_TRY(p->hq.alloc(hq_cap));
-    GC_TRY(p->hq_len.alloc(1));
-    GC_TRY(p->walk_elems.alloc(1));
-    GC_TRY(p->reasons.alloc(8));
-    const std::vector<int> order = te_tile_order(n);
-    GC_TRY(p->pair_order.alloc(order.size()));
-    GC_TRY_CUDA(cudaMemcpy(p->pair_order.p, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
+} // namespace
 
-    const int                  nblocks = (Nv + p->Q - 1) / p->Q;
-    std::vector<gc::TeParams>  all;
-    std::vector<long long>     pre;
-    for (int b = 0; b <= nblocks; ++b)
-    {
-        gc::TeParams d{};
-        d.X32        = p->X32.p;
-        d.XT         = p->XT.p;
-        d.eps_atom   = p->eps.p;
-        d.SG         = p->SG.p;
-        d.PG         = p->PG.p;
-        d.SM         = p->SM.p;
-        d.PM         = p->PM.p;
-        d.natoms     = n;
-        d.T          = p->T;
-        d.lag        = p->lag;
-        d.Nv         = Nv;
-        d.K          = p->K;
-        d.Lpad       = p->Lpad;
-        d.Qp         = p->Qp;
-        d.i0         = b < nblocks ? b * p->Q : 0;
-        d.Q          = b < nblocks ? std::min(p->Q, Nv - b * p->Q) : p->Q;
-        d.pair_count = p->npairs;
-        d.pair_order = p->pair_order.p;
-        d.shift      = gc::walk_histogram_shift(p->K);
-        d.cnt        = p->cnt.p;
-        d.wres       = p->wres.p;
-        d.hq         = p->hq.p;
-        d.hq_len     = p->hq_len.p;
-        d.hq_cap     = hq_cap;
-        d.status     = p->status.p;
-        d.walk_elems = p->walk_elems.p;
-        d.reasons    = p->reasons.p;
-        all.push_back(d); // the last one is the fix-up's descriptor
-        if (b < nblocks)
-        {
-            const long long grp = (d.Q + 31) / 32;
-            pre.insert(pre.end(), {0, 2LL * n * d.Q, 0, (grp + chunk - 1) / chunk * p->npairs, 0, grp * p->npairs});
-        }
-    }
-    GC_TRY(p->descs.alloc(all.size()));
-    GC_TRY(p->prefix.alloc(pre.size()));
-    GC_TRY(p->counters.alloc(2 * (size_t)nblocks));
-    GC_TRY_CUDA(cudaMemcpy(p->descs.p, all.data(), sizeof(gc::TeParams) * all.size(), cudaMemcpyHostToDevice));
-    GC_TRY_CUDA(cudaMemcpy(p->prefix.p, pre.data(), sizeof(long long) * pre.size(), cudaMemcpyHostToDevice));
-    p->waves.clear();
-    p->wave_rows.clear();
-    for (int b = 0; b < nblocks; ++b)
-    {
-        gc::TeBatch w{};
-        w.d       = p->descs.p + b;
-        w.rprefix = p->prefix.p + 6 * b;
-        w.wprefix = w.rprefix + 2;
-        w.fprefix = w.rprefix + 4;
-        w.n       = 1;
-        w.maxT    = p->T;
-        w.maxNv   = Nv;
-        w.maxK    = p->K;
-        w.chunk   = chunk;
-        w.counter = p->counters.p + 2 * b;
-        p->waves.push_back(w);
-        p->wave_rows.push_back(2LL * n * all[(size_t)b].Q);
-    }
-    p->fix       = gc::TeBatch{};
-    p->fix.d     = p->descs.p + nblocks;
-    p->fix.n     = 1;
-    p->fix.maxT  = p->T;
-    p->fix.maxNv = Nv;
-    p->fix.maxK  = p->K;
+namespace gc {
+namespace host {
+
+double te_row_bytes_per_query(int natoms, int Nv)
+{
+    // G and M rows of every atom: (distance + frame) per entry
+    return 2.0 * natoms * (double)(((Nv - 1) + 31) & ~31) * 6.0;
+}
+
+gc_status TeTraj::create(int n, int nframes, int k, int lg, int q)
+{
+    natoms = n;
+    T      = nframes;
+    K      = k;
+    lag    = lg;
+    Nv     = T - lag;
+    npairs = (long)n * (n - 1);
+    GC_TRY(XT.alloc((size_t)n * T * 3));
+    // psi[0 .. N_valid + 1]: a count clamped to N_valid indexes psi[N_valid + 1]
+    GC_TRY(psi.alloc((size_t)Nv + 2));
+    GC_TRY(X32.alloc((size_t)n * T));
+    GC_TRY(eps.alloc((size_t)n));
+    GC_TRY(cnt.alloc((size_t)Nv * npairs));
+    const std::vector<double> tab = digamma_table(Nv + 1);
+    GC_TRY_CUDA(cudaMemcpy(psi.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+    Q = q;
+    if (Q <= 0)
+        return GC_OK;
+    Qp   = (Q + 31) & ~31;
+    Lpad = ((Nv - 1) + 31) & ~31;
+    const size_t rows = (size_t)n * Qp * Lpad;
+    GC_TRY(SG.alloc(rows));
+    GC_TRY(SM.alloc(rows));
+    GC_TRY(PG.alloc(rows));
+    GC_TRY(PM.alloc(rows));
+    GC_TRY(wres.alloc((size_t)Q * npairs));
+    const double hq_want = 0.01 * (double)npairs * Nv + 4096.0;
+    hq_cap               = (unsigned)(hq_want < 16777216.0 ? hq_want : 16777216.0);
+    GC_TRY(hq.alloc(hq_cap));
+    GC_TRY(hq_len.alloc(1));
+    GC_TRY(walk_elems.alloc(1));
+    GC_TRY(reasons.alloc(8));
+    const std::vector<int> order = te_tile_order(n);
+    GC_TRY(pair_order.alloc(order.size()));
+    GC_TRY_CUDA(cudaMemcpy(pair_order.p, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
     return GC_OK;
 }
 
-} // namespace
+TeParams TeTraj::desc(int* status, int b) const
+{
+    TeParams d{};
+    d.X32        = X32.p;
+    d.XT         = XT.p;
+    d.eps_atom   = eps.p;
+    d.SG         = SG.p;
+    d.PG         = PG.p;
+    d.SM         = SM.p;
+    d.PM         = PM.p;
+    d.natoms     = natoms;
+    d.T          = T;
+    d.lag        = lag;
+    d.Nv         = Nv;
+    d.K          = K;
+    d.Lpad       = Lpad;
+    d.Qp         = Qp;
+    d.i0         = b * Q;
+    d.Q          = std::min(Q, Nv - b * Q);
+    d.pair_count = npairs;
+    d.pair_order = pair_order.p;
+    d.shift      = gc::walk_histogram_shift(K);
+    d.cnt        = cnt.p;
+    d.wres       = wres.p;
+    d.hq         = hq.p;
+    d.hq_len     = hq_len.p;
+    d.hq_cap     = hq_cap;
+    d.status     = status;
+    d.walk_elems = walk_elems.p;
+    d.reasons    = reasons.p;
+    return d;
+}
+
+gc_status TeTraj::prepare(const double* d_xyz, int* status, cudaStream_t s) const
+{
+    gc::launch_transpose_components(d_xyz, natoms, T, XT.p, status, s);
+    gc::launch_te_x32(XT.p, natoms, T, X32.p, eps.p, s);
+    if (Q > 0)
+    {
+        GC_TRY_CUDA(cudaMemsetAsync(hq_len.p, 0, sizeof(unsigned), s));
+        GC_TRY_CUDA(cudaMemsetAsync(reasons.p, 0, 8 * sizeof(unsigned), s));
+        GC_TRY_CUDA(cudaMemsetAsync(walk_elems.p, 0, sizeof(unsigned long long), s));
+    }
+    GC_TRY_CUDA(cudaGetLastError());
+    return GC_OK;
+}
+
+gc_status TeLaunch::build(const std::vector<std::vector<TeParams>>& wave_descs, const std::vector<TeParams>& traj_descs)
+{
+    int maxT = 0, maxNv = 0, maxK = 0;
+    for (const auto& wv : wave_descs)
+        for (const TeParams& d : wv)
+        {
+            maxT  = std::max(maxT, d.T);
+            maxNv = std::max(maxNv, d.Nv);
+            maxK  = std::max(maxK, d.K);
+        }
+    gc::walk_shape(maxT, &warps, &staged);
+    const long long        chunk = (long long)warps * 4;
+    std::vector<TeParams>  all;
+    std::vector<long long> pre;
+    std::vector<size_t>    dofs, pofs;
+    for (const auto& wv : wave_descs)
+    {
+        dofs.push_back(all.size());
+        pofs.push_back(pre.size());
+        std::vector<long long> rp{0}, wp{0}, fp{0};
+        for (const TeParams& d : wv)
+        {
+            all.push_back(d);
+            const long long grp = (d.Q + 31) / 32;
+            rp.push_back(rp.back() + 2LL * d.natoms * d.Q);
+            wp.push_back(wp.back() + (grp + chunk - 1) / chunk * d.pair_count);
+            fp.push_back(fp.back() + grp * d.pair_count);
+        }
+        pre.insert(pre.end(), rp.begin(), rp.end());
+        pre.insert(pre.end(), wp.begin(), wp.end());
+        pre.insert(pre.end(), fp.begin(), fp.end());
+    }
+    const size_t tofs = all.size();
+    all.insert(all.end(), traj_descs.begin(), traj_descs.end());
+    GC_TRY(descs.alloc(all.size()));
+    GC_TRY(prefix.alloc(pre.size()));
+    GC_TRY(counters.alloc(2 * wave_descs.size() + 1));
+    GC_TRY_CUDA(cudaMemcpy(descs.p, all.data(), sizeof(TeParams) * all.size(), cudaMemcpyHostToDevice));
+    GC_TRY_CUDA(cudaMemcpy(prefix.p, pre.data(), sizeof(long long) * pre.size(), cudaMemcpyHostToDevice));
+    waves.clear();
+    wave_rows.clear();
+    for (size_t v = 0; v < wave_descs.size(); ++v)
+    {
+        const int n = (int)wave_descs[v].size();
+        TeBatch   b{};
+        b.d       = descs.p + dofs[v];
+        b.rprefix = prefix.p + pofs[v];
+        b.wprefix = b.rprefix + (n + 1);
+        b.fprefix = b.wprefix + (n + 1);
+        b.n       = n;
+        b.maxT    = maxT;
+        b.maxNv   = maxNv;
+        b.maxK    = maxK;
+        b.chunk   = (int)chunk;
+        b.counter = counters.p + 2 * v;
+        waves.push_back(b);
+        wave_rows.push_back(pre[pofs[v] + n]);
+    }
+    fix       = TeBatch{};
+    fix.d     = descs.p + tofs;
+    fix.n     = (int)traj_descs.size();
+    fix.maxT  = maxT;
+    fix.maxNv = maxNv;
+    fix.maxK  = maxK;
+    return GC_OK;
+}
+
+gc_status TeLaunch::enqueue(int sms, cudaStream_t s)
+{
+    launches = 0;
+    if (!waves.empty())
+        GC_TRY_CUDA(cudaMemsetAsync(counters.p, 0, sizeof(unsigned long long) * 2 * waves.size(), s));
+    for (const TeBatch& w : waves)
+    {
+        GC_TRY_CUDA(gc::launch_te_rows(w, wave_rows[(size_t)(&w - waves.data())], s));
+        GC_TRY_CUDA(gc::launch_te_walk(w, warps, staged, sms, s));
+        GC_TRY_CUDA(gc::launch_te_finish(w, sms, s));
+        // the walk's task counter serves the count kernel
+        GC_TRY_CUDA(cudaMemsetAsync(w.counter, 0, sizeof(unsigned long long), s));
+        GC_TRY_CUDA(gc::launch_te_count(w, warps, staged, sms, s));
+        launches += 4;
+    }
+    if (fix.n > 0)
+    {
+        GC_TRY_CUDA(gc::launch_te_fixup(fix, sms, s));
+        launches += 2;
+    }
+    return GC_OK;
+}
+
+} // namespace host
+} // namespace gc
+
+struct gc_te_plan
+{
+    int                 device = 0, sms = 148;
+    int                 natoms = 0, T = 0, K = 0, lag = 0, Nv = 0, path = GC_PATH_AUTO;
+    long                npairs = 0; // ordered pairs
+    bool                walk   = false;
+    cudaStream_t        stream = nullptr;
+    cudaEvent_t         ev0 = nullptr, ev1 = nullptr, ev_done = nullptr;
+    gc::host::TeTraj    tt;
+    gc::host::TeLaunch  tl;
+    DevBuf<int>         status;
+    int                 launches = 0;
+    long                handoffs = 0;
+    double              walk_mean = 0.0;
+};
 
 extern "C" {
 
@@ -218,17 +294,24 @@ gc_status gc_te_plan_create(int natoms, int nframes, int k, int lag, const gc_op
     GC_TRY_CUDA(cudaEventCreate(&p->ev0));
     GC_TRY_CUDA(cudaEventCreate(&p->ev1));
     GC_TRY_CUDA(cudaEventCreateWithFlags(&p->ev_done, cudaEventDisableTiming));
-    GC_TRY(p->XT.alloc((size_t)natoms * nframes * 3));
-    // psi[0 .. N_valid + 1]: a count clamped to N_valid indexes psi[N_valid + 1]
-    GC_TRY(p->psi.alloc((size_t)p->Nv + 2));
-    GC_TRY(p->X32.alloc((size_t)natoms * nframes));
-    GC_TRY(p->eps.alloc((size_t)natoms));
-    GC_TRY(p->cnt.alloc((size_t)p->Nv * p->npairs));
     GC_TRY(p->status.alloc(1));
-    const std::vector<double> psi = digamma_table(p->Nv + 1);
-    GC_TRY_CUDA(cudaMemcpy(p->psi.p, psi.data(), sizeof(double) * psi.size(), cudaMemcpyHostToDevice));
+    int Q = 0;
     if (p->walk)
-        GC_TRY(te_build_walk(p.get()));
+    {
+        int  warps  = 0;
+        bool staged = false;
+        gc::walk_shape(nframes, &warps, &staged);
+        // sorted G and M rows of one query block within 16 GiB
+        Q = ksg_block_queries(2 * natoms, p->Nv, 16.0 * (1 << 30), 32 * warps);
+    }
+    GC_TRY(p->tt.create(natoms, nframes, k, lag, Q));
+    if (p->walk)
+    {
+        std::vector<std::vector<gc::TeParams>> waves;
+        for (int b = 0; b < p->tt.blocks(); ++b)
+            waves.push_back({p->tt.desc(p->status.p, b)});
+        GC_TRY(p->tl.build(waves, {p->tt.desc(p->status.p, 0)}));
+    }
     *out = p.release();
     return GC_OK;
 }
@@ -241,41 +324,26 @@ gc_status gc_te_plan_run(gc_te_plan* p, const double* d_xyz, double* d_te, void*
     GC_TRY(dev.st);
     cudaStream_t s = stream ? (cudaStream_t)stream : p->stream;
     const int    n = p->natoms;
-    p->launches    = 0;
     GC_TRY_CUDA(cudaMemsetAsync(p->status.p, 0, sizeof(int), s));
     GC_TRY_CUDA(cudaMemsetAsync(d_te, 0, sizeof(double) * (size_t)n * n, s));
-    gc::launch_transpose_components(d_xyz, n, p->T, p->XT.p, p->status.p, s);
-    gc::launch_te_x32(p->XT.p, n, p->T, p->X32.p, p->eps.p, s);
-    p->launches += 2;
+    GC_TRY(p->tt.prepare(d_xyz, p->status.p, s));
+    p->launches = 2;
     GC_TRY_CUDA(cudaEventRecord(p->ev0, s));
     if (p->walk)
     {
-        GC_TRY_CUDA(cudaMemsetAsync(p->counters.p, 0, sizeof(unsigned long long) * 2 * p->waves.size(), s));
-        GC_TRY_CUDA(cudaMemsetAsync(p->hq_len.p, 0, sizeof(unsigned), s));
-        GC_TRY_CUDA(cudaMemsetAsync(p->reasons.p, 0, 8 * sizeof(unsigned), s));
-        GC_TRY_CUDA(cudaMemsetAsync(p->walk_elems.p, 0, sizeof(unsigned long long), s));
-        for (size_t w = 0; w < p->waves.size(); ++w)
-        {
-            GC_TRY_CUDA(gc::launch_te_rows(p->waves[w], p->wave_rows[w], s));
-            GC_TRY_CUDA(gc::launch_te_walk(p->waves[w], p->warps, p->staged, p->sms, s));
-            GC_TRY_CUDA(gc::launch_te_finish(p->waves[w], p->sms, s));
-            GC_TRY_CUDA(cudaMemsetAsync(p->waves[w].counter, 0, sizeof(unsigned long long), s));
-            GC_TRY_CUDA(gc::launch_te_count(p->waves[w], p->warps, p->staged, p->sms, s));
-            p->launches += 4;
-        }
-        GC_TRY_CUDA(gc::launch_te_fixup(p->fix, p->sms, s));
+        GC_TRY(p->tl.enqueue(p->sms, s));
         GC_TRY_CUDA(cudaEventRecord(p->ev1, s));
-        GC_TRY_CUDA(gc::launch_te_reduce(p->cnt.p, n, p->Nv, p->K, p->psi.p, d_te, s));
-        p->launches += 3;
+        GC_TRY_CUDA(gc::launch_te_reduce(p->tt.cnt.p, n, p->Nv, p->K, p->tt.psi.p, d_te, s));
+        p->launches += p->tl.launches + 1;
     }
     else
     {
         if (p->path == GC_PATH_EXACT_FP64)
-            gc::launch_te_exact(p->XT.p, n, p->T, p->K, p->lag, p->cnt.p, s);
+            gc::launch_te_exact(p->tt.XT.p, n, p->T, p->K, p->lag, p->tt.cnt.p, s);
         else
-            gc::launch_te_fast(p->XT.p, p->X32.p, p->eps.p, n, p->T, p->K, p->lag, p->cnt.p, s);
+            gc::launch_te_fast(p->tt.XT.p, p->tt.X32.p, p->tt.eps.p, n, p->T, p->K, p->lag, p->tt.cnt.p, s);
         GC_TRY_CUDA(cudaEventRecord(p->ev1, s));
-        gc::launch_te_finalize(p->cnt.p, n, p->T, p->K, p->lag, p->psi.p, d_te, s);
+        gc::launch_te_finalize(p->tt.cnt.p, n, p->T, p->K, p->lag, p->tt.psi.p, d_te, s);
         p->launches += 2;
     }
     GC_TRY_CUDA(cudaGetLastError());
@@ -297,11 +365,11 @@ gc_status gc_te_plan_sync(gc_te_plan* p)
     if (p->walk)
     {
         unsigned rc[8] = {};
-        GC_TRY_CUDA(cudaMemcpy(rc, p->reasons.p, sizeof(rc), cudaMemcpyDeviceToHost));
+        GC_TRY_CUDA(cudaMemcpy(rc, p->tt.reasons.p, sizeof(rc), cudaMemcpyDeviceToHost));
         for (unsigned r : rc)
             p->handoffs += (long)r;
         unsigned long long we = 0;
-        GC_TRY_CUDA(cudaMemcpy(&we, p->walk_elems.p, sizeof(we), cudaMemcpyDeviceToHost));
+        GC_TRY_CUDA(cudaMemcpy(&we, p->tt.walk_elems.p, sizeof(we), cudaMemcpyDeviceToHost));
         p->walk_mean = (double)we / ((double)p->npairs * p->Nv);
     }
     return status_to_error(st & gc::kStatNonFinite);
@@ -340,11 +408,11 @@ gc_status gc_te_plan_counts(gc_te_plan* p, int a1, int a2, int32_t* n_xp, int32_
     const long q = (long)a1 * (p->natoms - 1) + (a2 < a1 ? a2 : a2 - 1);
     std::vector<uint2> c((size_t)p->Nv);
     if (p->walk) // pair-major [q][Nv]
-        GC_TRY_CUDA(cudaMemcpy(c.data(), p->cnt.p + (size_t)q * p->Nv, sizeof(uint2) * c.size(),
+        GC_TRY_CUDA(cudaMemcpy(c.data(), p->tt.cnt.p + (size_t)q * p->Nv, sizeof(uint2) * c.size(),
                                cudaMemcpyDeviceToHost));
     else // query-major [qi][npairs]
-        GC_TRY_CUDA(cudaMemcpy2D(c.data(), sizeof(uint2), p->cnt.p + q, sizeof(uint2) * p->npairs, sizeof(uint2),
-                                 (size_t)p->Nv, cudaMemcpyDeviceToHost));
+        GC_TRY_CUDA(cudaMemcpy2D(c.data(), sizeof(uint2), p->tt.cnt.p + q, sizeof(uint2) * p->npairs,
+                                 sizeof(uint2), (size_t)p->Nv, cudaMemcpyDeviceToHost));
     for (int i = 0; i < p->Nv; ++i)
     {
         if (n_xp)

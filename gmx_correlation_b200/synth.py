@@ -23,7 +23,7 @@ from __future__ import annotations
 
 import numpy as np
 
-__all__ = ["raw_positions", "center", "synth_traj", "CONFIGS"]
+__all__ = ["raw_positions", "center", "synth_traj", "CONFIGS", "batch_specs"]
 
 # Generator settings of the reference-shaped workloads.
 CONFIGS = {
@@ -82,3 +82,22 @@ def synth_traj(natoms: int, nframes: int, n_modes: int = 8, sigma_l: float = 0.0
 def config_traj(name: str) -> np.ndarray:
     c = CONFIGS[name]
     return synth_traj(c["natoms"], c["nframes"], c["n_modes"], c["sigma_l"], c["seed"], c["fp32"])
+
+
+def batch_specs(count: int = 16, seed: int = 3):
+    """The batched uneven workload: `count` independent trajectories with
+    atoms uniform in [50, 400], frames uniform in [500, 4000] and k drawn from
+    {10, 50, 100}; each entry holds the generator settings of one trajectory
+    (16 latent modes, loadings 0.08 nm, float32-rounded positions, its own
+    seed)."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for i in range(count):
+        out.append(dict(natoms=int(rng.integers(50, 401)), nframes=int(rng.integers(500, 4001)),
+                        k=int(rng.choice([10, 50, 100])), n_modes=16, sigma_l=0.08, fp32=True,
+                        seed=1000 * seed + i))
+    return out
+
+
+def batch_traj(spec: dict) -> np.ndarray:
+    return synth_traj(spec["natoms"], spec["nframes"], spec["n_modes"], spec["sigma_l"], spec["seed"], spec["fp32"])

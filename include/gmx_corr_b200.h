@@ -144,6 +144,30 @@ void      gc_ksg_batch_release(void);
  * (lib/correlation_core.h:76, lib/correlation_core.cpp:280-311). */
 gc_status gc_gauss_matrix(const gc_traj_view* traj, const gc_opts* opts, double* mi);
 
+/* Transfer-entropy matrices of ntraj trajectories at one lag in one batched
+ * run: trajectory i (its own atom and frame counts, nframes - lag <= 16385)
+ * with k = ks[i] into te[i] (natoms_i * natoms_i, the conventions of
+ * gc_te_matrix; all zeros when nframes - lag <= k, as in the reference).
+ * The query blocks of all trajectories share each launch of the row sort,
+ * walk, finish and count kernels, and the sequence runs as a captured CUDA
+ * graph; the workspace and graph of the last batch (shapes and lag) are
+ * kept for a repeated call (gc_te_batch_release frees them; the per-query
+ * counts take 8 bytes per ordered pair and frame, about 22 GB for 16
+ * trajectories of up to 400 atoms x 4000 frames, beside up to 24 GiB of
+ * sorted rows).  No counterpart in the reference, which computes te_matrix
+ * per trajectory.  opts: device only. */
+gc_status gc_te_batch(const gc_traj_view* trajs, const int* ks, int ntraj, int lag, const gc_opts* opts,
+                      double* const* te);
+void      gc_te_batch_release(void);
+
+/* Gaussian-copula MI matrices of ntraj trajectories (nframes <= 16384 each)
+ * in one captured CUDA graph, with the conventions of gc_gcmi_matrix.  The
+ * last batch's workspace and graph are kept for a repeated call with the
+ * same shapes; gc_gcmi_batch_release frees them.  No counterpart in the
+ * reference (gcmi_corrmatrix is per trajectory).  opts: device only. */
+gc_status gc_gcmi_batch(const gc_traj_view* trajs, int ntraj, const gc_opts* opts, double* const* mi);
+void      gc_gcmi_batch_release(void);
+
 /* Gaussian-copula MI matrix.  Replaces gcmi_corrmatrix (lib/gcmi.h:8-9,
  * lib/gcmi.cpp:246-317). */
 gc_status gc_gcmi_matrix(const gc_traj_view* traj, const gc_opts* opts, double* mi);

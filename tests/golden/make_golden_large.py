@@ -26,6 +26,11 @@ Fixtures:
             of 600 x 4000 (seed 11) and 1000 x 5000 (seed 5), k = 100.
   variants  whole KSG matrices and per-pair count digests of the row-length
             and k variants (3000 / 5000 / 9000-frame rows, k = 300).
+  batch     the batched uneven workload (synth.batch_specs: 16 trajectories,
+            50-400 atoms, 500-4000 frames, k in {10, 50, 100}): per
+            trajectory the KSG MI and count digest of 2 seeded pairs, the
+            reference's GCMI of those pairs, and TE at lags 1 / 5 / 10 of both
+            orders of one pair (two-atom te_matrix, as for te247).
 
 A count digest is the first 16 hex digits of sha256(nx as int32 || ny as
 int32), so a 5000-frame pair costs 16 bytes instead of 40 KB.
@@ -45,7 +50,7 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT))
 
-from gmx_correlation_b200.synth import CONFIGS, config_traj, synth_traj  # noqa: E402
+from gmx_correlation_b200.synth import CONFIGS, batch_specs, batch_traj, config_traj, synth_traj  # noqa: E402
 from oracle import Oracle, Reference  # noqa: E402
 
 # Shapes of the sampled-size and variant fixtures (atoms, frames, modes,
@@ -172,12 +177,42 @@ def make_variants(ref):
     np.savez_compressed(HERE / "variants.npz", **out)
 
 
+def make_batch(ref):
+    out = {}
+    t0 = time.time()
+    for i, sp in enumerate(batch_specs()):
+        x = batch_traj(sp)
+        n, k = sp["natoms"], sp["k"]
+        pairs = seeded_pairs(n, 2, 500 + i)
+        mi, dig = [], []
+        for a1, a2 in pairs:
+            d = ref.ksg_pair_detail(x, k, a1, a2)
+            mi.append(d["mi"])
+            dig.append(count_digest(d["nx"], d["ny"]))
+        g = ref.gcmi_matrix(x)
+        a1, a2 = pairs[0]
+        te = np.zeros((3, 2))
+        for li, lag in enumerate((1, 5, 10)):
+            m = ref.te_matrix(np.ascontiguousarray(x[[a1, a2]]), k, lag)
+            te[li] = (m[0, 1], m[1, 0])  # TE(a2 -> a1), TE(a1 -> a2)
+        out[f"b{i}_sha256"] = coords_sha(x)
+        out[f"b{i}_pairs"] = np.array(pairs, np.int32)
+        out[f"b{i}_ksg"] = np.array(mi)
+        out[f"b{i}_count_digest"] = np.array(dig)
+        out[f"b{i}_gcmi"] = np.array([g[p1, p2] for p1, p2 in pairs])
+        out[f"b{i}_te"] = te
+        print(f"batch {i}: {n}x{sp['nframes']} k={k} ({time.time() - t0:.0f} s)", flush=True)
+    np.savez_compressed(HERE / "batch.npz", lags=np.array([1, 5, 10]), **out)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--only", nargs="*", default=None, help="subset of: ref247 te247 sizes variants")
+    ap.add_argument("--only", nargs="*", default=None, help="subset of: ref247 te247 sizes variants batch")
     a = ap.parse_args(argv)
-    want = set(a.only or ["variants", "sizes", "te247", "ref247"])
+    want = set(a.only or ["variants", "sizes", "te247", "batch", "ref247"])
     ref, orc = Reference(), Oracle()
+    if "batch" in want:
+        make_batch(ref)
     if "variants" in want:
         make_variants(ref)
     if "sizes" in want:

@@ -61,7 +61,11 @@ def _free_port():
     return port
 
 
-def test_two_gloo_ranks_rebuild_the_reference_matrix(oracle):
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_rebuild_the_reference_matrix(oracle, world):
+    """Each rank computes its shard; the all-gather of the packed pair values
+    (uneven shards with three ranks: 36 pairs) rebuilds the reference's matrix
+    on every rank."""
     from gmx_correlation_b200.synth import synth_traj
     x = synth_traj(9, 160, 4, 0.08, seed=77)
     k = 6
@@ -69,15 +73,26 @@ def test_two_gloo_ranks_rebuild_the_reference_matrix(oracle):
     manager = ctx.Manager()
     out = manager.dict()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, x, k, out)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, x, k, out)) for r in range(world)]
     for p in procs:
         p.start()
     for p in procs:
         p.join(timeout=120)
         assert p.exitcode == 0
     want = oracle.ksg_matrix(x, k)
-    for r in range(2):
+    for r in range(world):
         np.testing.assert_array_equal(out[r], want)
+
+
+def test_pairs_to_matrix_layout():
+    from gmx_correlation_b200.shard import pairs_to_matrix
+    n = 7
+    v = np.arange(n * (n - 1) // 2, dtype=float) + 1.0
+    m = pairs_to_matrix(v, n)
+    for p in range(len(v)):
+        a1, a2 = pair_of(p)
+        assert m[a1, a2] == m[a2, a1] == v[p]
+    assert np.all(np.diag(m) == 2000.0)
 
 
 def test_single_rank_reduce_is_identity():

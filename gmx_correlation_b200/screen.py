@@ -10,6 +10,11 @@ BF16 tensor-core kernels.  numpy does only the bookkeeping (sampling, the
 
     python -m gmx_correlation_b200.screen train --out screen_model.npz
     python -m gmx_correlation_b200.screen eval --model screen_model.npz
+    python -m gmx_correlation_b200.screen study > study.json
+
+`study` measures, on the 247 x 2000, k = 100 workload, how many pairs any
+affordable predictor could leave to its prediction at audited max
+|dr| <= 1e-2, and what that would save (see study()).
 """
 
 from __future__ import annotations
@@ -175,6 +180,112 @@ def train_screen(raw, r, tid, *, members=4, epochs=40, batch=1024, lr=2e-3, seed
     return TrainedScreen(model, fmean, fsd, pca, meta)
 
 
+def _plan_ms(x, k, device=-1, reps=3):
+    """Device time (CUDA events) of the KSG neighbour kernels for one matrix."""
+    import torch
+
+    from . import KsgPlan
+    n, T = x.shape[0], x.shape[1]
+    d_xyz = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    plan = KsgPlan(n, T, k, device=device)
+    out = torch.zeros(plan.pairs, dtype=torch.float64, device="cuda")
+    ms = []
+    for _ in range(reps + 1):
+        plan.run(d_xyz.data_ptr(), out.data_ptr())
+        plan.sync()
+        ms.append(plan.kernel_ms)
+    plan.close()
+    return float(np.median(ms[1:]))
+
+
+def _packed(mat):
+    n = mat.shape[0]
+    a1, a2 = np.tril_indices(n, -1)
+    return mat[a1, a2]
+
+
+def _err_stats(err, tol):
+    a = np.abs(err)
+    return {"rms": float(np.sqrt(np.mean(err ** 2))), "q50": float(np.quantile(a, 0.5)),
+            "q99": float(np.quantile(a, 0.99)), "q999": float(np.quantile(a, 0.999)), "max": float(a.max()),
+            "within_tol": float(np.mean(a <= tol))}
+
+
+def study(model_path=DEFAULT_MODEL, k=100, tol=1e-2, coverage=0.999, audit_frac=0.05, seed=5, device=-1):
+    """How far can screening go at audited max |dr| <= tol on the reference-size
+    workload (247 x 2000, k = 100)?
+
+    Predictors of the exact KSG r, from cheapest: the committed MLP ensemble
+    (features + network, about 2 ms); KSG with k = 25 and k = 10 on the same
+    frames; KSG with k = 50 on every second frame.  For each: its error
+    distribution against exact k = 100 KSG over all 30,381 pairs, and
+    `within_tol`, the fraction of pairs whose error is within tol (the most
+    any rule could keep, even one that knew every error).  Then the best
+    practical rule: a linear model of r on every predictor, fitted on a random
+    half of the pairs, whose residual quantile at `coverage` is calibrated per
+    bin of the predictors' disagreement (|r_k25 - r_mlp|) on that half and
+    applied to the other half (conformal, split by pairs).  The reported
+    speed-up of a screened matrix counts the predictors' cost, exact KSG on
+    the pairs the rule does not keep and on the audit sample."""
+    import torch  # noqa: F401  (KsgPlan device buffers)
+
+    from .synth import config_traj
+    x = config_traj("ref")
+    ts = TrainedScreen.load(model_path, device)
+    out = {"workload": "247 atoms x 2000 frames, k=100 (the bench matrix)", "tol": tol, "coverage": coverage}
+    r100 = r_of_mi(_packed(kraskov_corrmatrix(x, k, device=device)))
+    t100 = _plan_ms(x, k, device)
+    cand = {}
+    t0 = time.perf_counter()
+    F = screen_features(x, k, pca=ts.pca, device=device)
+    Y = ts.model.predict(F)
+    t_mlp = (time.perf_counter() - t0) * 1e3
+    cand["mlp"] = (Y.mean(0), t_mlp)
+    for kk in (25, 10):
+        cand[f"ksg_k{kk}"] = (r_of_mi(_packed(kraskov_corrmatrix(x, kk, device=device))), _plan_ms(x, kk, device))
+    xs = np.ascontiguousarray(x[:, ::2])
+    cand["ksg_half_frames_k50"] = (r_of_mi(_packed(kraskov_corrmatrix(xs, k // 2, device=device))),
+                                   _plan_ms(xs, k // 2, device))
+    out["exact_ms"] = t100
+    out["spread_vs_error_spearman"] = float(np.corrcoef(np.argsort(np.argsort(Y.std(0))),
+                                                       np.argsort(np.argsort(np.abs(Y.mean(0) - r100))))[0, 1])
+    out["predictors"] = {name: dict(_err_stats(r - r100, tol), cost_ms=c, cost_vs_exact=c / t100)
+                         for name, (r, c) in cand.items()}
+    # the best practical rule: linear model on every predictor + conformal bins
+    rng = np.random.default_rng(seed)
+    P = len(r100)
+    A = np.zeros(P, bool)
+    A[rng.choice(P, P // 2, replace=False)] = True
+    B = ~A
+    X = np.column_stack([np.ones(P)] + [r for r, _ in cand.values()])
+    coef, *_ = np.linalg.lstsq(X[A], r100[A], rcond=None)
+    pred = X @ coef
+    res = pred - r100
+    dis = np.abs(cand["ksg_k25"][0] - cand["mlp"][0])
+    edges = np.quantile(dis[A], np.linspace(0, 1, 11))
+    keep = np.zeros(P, bool)
+    bins = []
+    for b in range(10):
+        inA = A & (dis >= edges[b]) & (dis <= edges[b + 1])
+        inB = B & (dis >= edges[b]) & (dis <= edges[b + 1])
+        qb = float(np.quantile(np.abs(res[inA]), coverage)) if inA.any() else np.inf
+        bins.append({"disagreement_max": float(edges[b + 1]), "residual_quantile": qb})
+        if qb <= tol:
+            keep |= inB
+    cost = sum(c for _, c in cand.values())
+    kept = float(keep[B].mean())
+    out["combined"] = dict(_err_stats(res[B], tol), cost_ms=cost, bins=bins, kept_fraction=kept,
+                           kept_max_dr=float(np.abs(res[keep]).max()) if keep.any() else 0.0)
+    exact_share = (1.0 - kept) + kept * audit_frac
+    out["combined"]["screened_ms"] = cost + exact_share * t100
+    out["combined"]["speedup_vs_plain"] = t100 / out["combined"]["screened_ms"]
+    # the ceiling with the cheapest predictor alone: keep every pair whose MLP
+    # error is within tol (needs an error oracle no rule has)
+    f = out["predictors"]["mlp"]["within_tol"]
+    out["mlp_oracle_ceiling_speedup"] = t100 / (t_mlp + ((1 - f) + f * audit_frac) * t100)
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -192,7 +303,12 @@ def main(argv=None):
     e.add_argument("--natoms", type=int, default=600)
     e.add_argument("--nframes", type=int, default=4000)
     e.add_argument("--k", type=int, default=100)
+    s = sub.add_parser("study")
+    s.add_argument("--model", default=str(DEFAULT_MODEL))
     a = ap.parse_args(argv)
+    if a.cmd == "study":
+        print(json.dumps(study(a.model)))
+        return
     if a.cmd == "train":
         print(f"generating {a.ntraj} trajectories ...", flush=True)
         raw, r, tid, _ = build_dataset(a.ntraj, a.pairs, a.k, a.seed)

@@ -267,9 +267,19 @@ def screened_variant(gc, x, k, plain_e2e_s: float, device: int, reps: int = 3):
                    "target_max_dr": 1e-2}
     loose = run(sigma_max=float("inf"), margin=0.0)
     loose["rule"] = {"sigma_max": "inf", "margin": 0.0, "audit_frac": 0.05}
-    return {"model": {k2: ts.meta[k2] for k2 in ("trajectories", "train_pairs", "calib_rms", "gauss_rms",
-                                                 "calib_accept_frac") if k2 in ts.meta},
-            "calibrated_1e-2": cal, "audit_only": loose}
+    out = {"model": {k2: ts.meta[k2] for k2 in ("trajectories", "train_pairs", "calib_rms", "gauss_rms",
+                                                "calib_accept_frac") if k2 in ts.meta},
+           "calibrated_1e-2": cal, "audit_only": loose}
+    # what any affordable predictor could do at the bar (gmx_correlation_b200.screen.study)
+    from gmx_correlation_b200.screen import study
+    st = study(device=device)
+    out["study"] = {"exact_ms": st["exact_ms"], "spread_vs_error_spearman": st["spread_vs_error_spearman"],
+                    "mlp_error": {k2: st["predictors"]["mlp"][k2] for k2 in ("rms", "q999", "max", "within_tol")},
+                    "mlp_oracle_ceiling_speedup": st["mlp_oracle_ceiling_speedup"],
+                    "rules": {name: [{k2: r[k2] for k2 in ("tol", "rms", "q999", "max", "kept_fraction",
+                                                             "kept_max_dr", "cost_ms", "speedup_vs_plain")}
+                                     for r in rules] for name, rules in st["rules"].items()}}
+    return out
 
 
 def large_variant(gc, torch, dev, local: int, mix_ops: float):

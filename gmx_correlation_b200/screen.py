@@ -251,38 +251,49 @@ def study(model_path=DEFAULT_MODEL, k=100, tol=1e-2, coverage=0.999, audit_frac=
                                                        np.argsort(np.argsort(np.abs(Y.mean(0) - r100))))[0, 1])
     out["predictors"] = {name: dict(_err_stats(r - r100, tol), cost_ms=c, cost_vs_exact=c / t100)
                          for name, (r, c) in cand.items()}
-    # the best practical rule: linear model on every predictor + conformal bins
+    # device cost of the MLP path (features + network), from the screened run's report
+    _, rep = ksg_screened(x, k, ts.model, sigma_max=float("inf"), margin=0.0, device=device)
+    out["predictors"]["mlp"]["cost_ms"] = rep["ms_features"] + rep["ms_mlp"]
+    out["predictors"]["mlp"]["cost_vs_exact"] = out["predictors"]["mlp"]["cost_ms"] / t100
+    costs = {name: out["predictors"][name]["cost_ms"] for name in cand}
+    # practical rules: a linear model of r on a set of predictors, fitted on a
+    # random half of the pairs; its residual quantile at `coverage` is
+    # calibrated on that half per decile of the predictors' disagreement and
+    # the pairs of the other half in deciles whose quantile is within tol are
+    # kept (split conformal by pairs)
     rng = np.random.default_rng(seed)
     P = len(r100)
     A = np.zeros(P, bool)
     A[rng.choice(P, P // 2, replace=False)] = True
     B = ~A
-    X = np.column_stack([np.ones(P)] + [r for r, _ in cand.values()])
-    coef, *_ = np.linalg.lstsq(X[A], r100[A], rcond=None)
-    pred = X @ coef
-    res = pred - r100
-    dis = np.abs(cand["ksg_k25"][0] - cand["mlp"][0])
-    edges = np.quantile(dis[A], np.linspace(0, 1, 11))
-    keep = np.zeros(P, bool)
-    bins = []
-    for b in range(10):
-        inA = A & (dis >= edges[b]) & (dis <= edges[b + 1])
-        inB = B & (dis >= edges[b]) & (dis <= edges[b + 1])
-        qb = float(np.quantile(np.abs(res[inA]), coverage)) if inA.any() else np.inf
-        bins.append({"disagreement_max": float(edges[b + 1]), "residual_quantile": qb})
-        if qb <= tol:
-            keep |= inB
-    cost = sum(c for _, c in cand.values())
-    kept = float(keep[B].mean())
-    out["combined"] = dict(_err_stats(res[B], tol), cost_ms=cost, bins=bins, kept_fraction=kept,
-                           kept_max_dr=float(np.abs(res[keep]).max()) if keep.any() else 0.0)
-    exact_share = (1.0 - kept) + kept * audit_frac
-    out["combined"]["screened_ms"] = cost + exact_share * t100
-    out["combined"]["speedup_vs_plain"] = t100 / out["combined"]["screened_ms"]
-    # the ceiling with the cheapest predictor alone: keep every pair whose MLP
-    # error is within tol (needs an error oracle no rule has)
+
+    def rule(names, tol_):
+        X = np.column_stack([np.ones(P)] + [cand[nm][0] for nm in names])
+        coef, *_ = np.linalg.lstsq(X[A], r100[A], rcond=None)
+        res = X @ coef - r100
+        dis = np.abs(cand[names[-1]][0] - cand[names[0]][0]) if len(names) > 1 else np.zeros(P)
+        edges = np.quantile(dis[A], np.linspace(0, 1, 11))
+        keep = np.zeros(P, bool)
+        for b in range(10):
+            inA = A & (dis >= edges[b]) & (dis <= edges[b + 1])
+            inB = B & (dis >= edges[b]) & (dis <= edges[b + 1])
+            if inA.any() and np.quantile(np.abs(res[inA]), coverage) <= tol_:
+                keep |= inB
+        cost = sum(costs[nm] for nm in names)
+        kept = float(keep[B].mean())
+        exact_share = (1.0 - kept) + kept * audit_frac
+        return dict(_err_stats(res[B], tol_), tol=tol_, cost_ms=cost, kept_fraction=kept,
+                    kept_max_dr=float(np.abs(res[keep]).max()) if keep.any() else 0.0,
+                    speedup_vs_plain=t100 / (cost + exact_share * t100))
+
+    out["rules"] = {}
+    for names in (["mlp"], ["mlp", "ksg_half_frames_k50"], list(cand)):
+        key = "+".join(names)
+        out["rules"][key] = [rule(names, t) for t in (tol, 0.015, 0.02, 0.03)]
+    # the ceiling of the cheapest predictor: keep every pair whose MLP error is
+    # within tol (it needs an error oracle no rule has)
     f = out["predictors"]["mlp"]["within_tol"]
-    out["mlp_oracle_ceiling_speedup"] = t100 / (t_mlp + ((1 - f) + f * audit_frac) * t100)
+    out["mlp_oracle_ceiling_speedup"] = t100 / (costs["mlp"] + ((1 - f) + f * audit_frac) * t100)
     return out
 
 

@@ -147,6 +147,7 @@ struct gc_ksg_plan
     int              launches = 0;
     cudaEvent_t      ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t      ev_done = nullptr; // recorded after the last kernel of a run, on the run's stream
+    bool             wide    = false;   // counts above 16 bits: n_x and n_y in two planes of cnt
     // fast path workspace
     bool                  fast = false;
     gc::host::KsgTraj     ft;
@@ -170,8 +171,8 @@ gc_status validate_ksg(int natoms, int T, int k, const gc_opts& o, long* pb, lon
         return fail(GC_ERR_INVALID, "kraskov_corrmatrix: nframes must exceed k (number of nearest neighbours)");
     if (k < 1)
         return fail(GC_ERR_INVALID, "kraskov_corrmatrix: k must be at least 1");
-    if (T > 65535)
-        return fail(GC_ERR_INVALID, "kraskov_corrmatrix: this build supports at most 65535 frames");
+    if (T > gc::kMaxFrames)
+        return fail(GC_ERR_INVALID, "kraskov_corrmatrix: this build supports at most 16777216 frames");
     if (o.variant != GC_VARIANT_DEFAULT && o.variant != GC_VARIANT_HBM_GATHER)
         return fail(GC_ERR_INVALID, "unknown gc_opts.variant");
     const long np = (long)natoms * (natoms - 1) / 2;
@@ -256,7 +257,10 @@ gc_status gc_ksg_plan_create(int natoms, int nframes, int k, const gc_opts* opts
     GC_TRY_CUDA(cudaEventCreateWithFlags(&p->ev_done, cudaEventDisableTiming));
     GC_TRY(p->X.alloc((size_t)3 * natoms * nframes));
     GC_TRY(p->psi.alloc((size_t)nframes + 1));
-    GC_TRY(p->cnt.alloc((size_t)nframes * (size_t)(pc > 0 ? pc : 1)));
+    // more than 65535 frames: counts need 32 bits each (the exact kernels'
+    // wide layout; the fast path stops at 16385 frames anyway)
+    p->wide = nframes > 65535;
+    GC_TRY(p->cnt.alloc((size_t)nframes * (size_t)(pc > 0 ? pc : 1) * (p->wide ? 2 : 1)));
     GC_TRY(p->status.alloc(1));
     GC_TRY_CUDA(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, p->device));
     // The fast path sorts each marginal row in shared memory (<= 16384
@@ -333,11 +337,13 @@ gc_status plan_run(gc_ksg_plan* p, const double* d_xyz, double* d_pair_mi, cudaS
         }
         else
         {
-            gc::launch_ksg_exact(p->X.p, p->T, p->K, p->pair_begin, p->pair_count, p->cnt.p, s, p->pair_ab.p);
+            gc::launch_ksg_exact(p->X.p, p->T, p->K, p->pair_begin, p->pair_count, p->cnt.p, s, p->pair_ab.p,
+                                 p->wide ? p->cnt.p + (size_t)p->T * p->pair_count : nullptr);
             p->launches += 1;
         }
         GC_TRY_CUDA(cudaEventRecord(p->ev1, s));
-        gc::launch_ksg_finalize(p->cnt.p, p->pair_count, p->T, p->K, p->psi.p, d_pair_mi, s);
+        gc::launch_ksg_finalize(p->cnt.p, p->pair_count, p->T, p->K, p->psi.p, d_pair_mi, s,
+                                p->wide ? p->cnt.p + (size_t)p->T * p->pair_count : nullptr);
         p->launches += 1;
     }
     GC_TRY_CUDA(cudaGetLastError());
@@ -571,18 +577,19 @@ gc_status ksg_matrix_impl(const gc_traj_view* traj, const double* X, const doubl
         GC_TRY_CUDA(cudaMemcpy(pm.data(), plan->io_mi.p, sizeof(double) * pc, cudaMemcpyDeviceToHost));
     if (o.detail_nx || o.detail_ny)
     {
-        std::vector<uint32_t> c((size_t)T * pc);
+        const bool            wide = plan->wide;
+        const size_t          m    = (size_t)T * pc;
+        std::vector<uint32_t> c(m * (wide ? 2 : 1));
         if (pc > 0)
             GC_TRY_CUDA(cudaMemcpy(c.data(), plan->cnt.p, sizeof(uint32_t) * c.size(), cudaMemcpyDeviceToHost));
-        for (long pl = 0; pl < pc; ++pl)
-            for (int i = 0; i < T; ++i)
-            {
-                const uint32_t v = c[(size_t)pl * T + i];
-                if (o.detail_nx)
-                    o.detail_nx[(size_t)pl * T + i] = (int32_t)(v & 0xFFFFu);
-                if (o.detail_ny)
-                    o.detail_ny[(size_t)pl * T + i] = (int32_t)(v >> 16);
-            }
+        for (size_t e = 0; e < m; ++e)
+        {
+            const uint32_t v = c[e];
+            if (o.detail_nx)
+                o.detail_nx[e] = (int32_t)(wide ? v : (v & 0xFFFFu));
+            if (o.detail_ny)
+                o.detail_ny[e] = (int32_t)(wide ? c[m + e] : (v >> 16));
+        }
     }
     // kraskov_corrmatrix: zero fill, diagonal 2000, symmetric entries.
     std::memset(mi, 0, sizeof(double) * (size_t)n * n);
@@ -631,8 +638,8 @@ static gc_status gauss_like(const gc_traj_view* traj, const gc_opts* opts, doubl
             return fail(GC_ERR_INVALID, "gcmi_corrmatrix: need at least 2 atoms");
         if (T < 6)
             return fail(GC_ERR_INVALID, "gcmi_corrmatrix: need at least 6 frames for a non-singular 6x6 covariance");
-        if (T > 16384)
-            return fail(GC_ERR_INVALID, "gcmi_corrmatrix: this build supports at most 16384 frames");
+        if (T > gc::kMaxFrames)
+            return fail(GC_ERR_INVALID, "gcmi_corrmatrix: this build supports at most 16777216 frames");
     }
     else if (n < 1 || T < 1)
         return fail(GC_ERR_INVALID, "gauss_corrmatrix: empty trajectory");
@@ -750,12 +757,13 @@ gc_status gc_ksg_pair(const double* rows6, int nframes, int k, const double* psi
     GC_TRY(d_X.alloc((size_t)6 * T));
     GC_TRY(d_psi.alloc((size_t)T + 1));
     GC_TRY(d_mi.alloc(1));
-    GC_TRY(d_cnt.alloc((size_t)T));
+    const bool wide = T > 65535;
+    GC_TRY(d_cnt.alloc((size_t)T * (wide ? 2 : 1)));
     GC_TRY_CUDA(cudaMemcpyAsync(d_X.p + (size_t)3 * T, rows6, sizeof(double) * 3 * T, cudaMemcpyHostToDevice, ss.s));
     GC_TRY_CUDA(cudaMemcpyAsync(d_X.p, rows6 + (size_t)3 * T, sizeof(double) * 3 * T, cudaMemcpyHostToDevice, ss.s));
     GC_TRY_CUDA(cudaMemcpyAsync(d_psi.p, psi, sizeof(double) * (T + 1), cudaMemcpyHostToDevice, ss.s));
-    gc::launch_ksg_exact(d_X.p, T, k, 0, 1, d_cnt.p, ss.s);
-    gc::launch_ksg_finalize(d_cnt.p, 1, T, k, d_psi.p, d_mi.p, ss.s);
+    gc::launch_ksg_exact(d_X.p, T, k, 0, 1, d_cnt.p, ss.s, nullptr, wide ? d_cnt.p + T : nullptr);
+    gc::launch_ksg_finalize(d_cnt.p, 1, T, k, d_psi.p, d_mi.p, ss.s, wide ? d_cnt.p + T : nullptr);
     GC_TRY_CUDA(cudaGetLastError());
     GC_TRY_CUDA(cudaMemcpyAsync(mi, d_mi.p, sizeof(double), cudaMemcpyDeviceToHost, ss.s));
     GC_TRY_CUDA(cudaStreamSynchronize(ss.s));

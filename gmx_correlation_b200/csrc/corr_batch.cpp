@@ -367,8 +367,8 @@ gc_status gc_gcmi_batch(const gc_traj_view* trajs, int ntraj, const gc_opts* opt
             return fail(GC_ERR_INVALID, "gcmi_corrmatrix: need at least 2 atoms");
         if (trajs[i].nframes < 6)
             return fail(GC_ERR_INVALID, "gcmi_corrmatrix: need at least 6 frames for a non-singular 6x6 covariance");
-        if (trajs[i].nframes > 16384)
-            return fail(GC_ERR_INVALID, "gcmi_corrmatrix: this build supports at most 16384 frames");
+        if (trajs[i].nframes > gc::kMaxFrames)
+            return fail(GC_ERR_INVALID, "gcmi_corrmatrix: this build supports at most 16777216 frames");
     }
     DeviceScope dev(o.device);
     GC_TRY(dev.st);

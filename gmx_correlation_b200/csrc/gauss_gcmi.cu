@@ -94,6 +94,9 @@ __global__ void probit_table_kernel(int T, double* __restrict__ zt)
     zt[t]          = __dmul_rn(sqrt(2.0), acklam_erfinv(__dsub_rn(__dmul_rn(2.0, p), 1.0)));
 }
 
+// Longest series the shared-memory sort below takes (next_pow2(T) * 12 bytes).
+constexpr int kCopulaSortMax = 16384;
+
 // One CTA per component: bitonic sort of (value, frame) in shared memory,
 // then midrank averaging of the probit scores over runs of equal values
 // (lib/gcmi.cpp:113-143).  Requires next_pow2(T) * 12 bytes of shared memory.
@@ -146,6 +149,43 @@ __global__ void copula_kernel(const double* __restrict__ XF, int natoms, int T, 
         for (int t = r; t < s; ++t)
             Z[(size_t)idx[t] * nc + comp] = avg;
     }
+}
+
+// The same copula scores for series too long to sort in shared memory: a
+// frame's run of equal values starts at rank r = #{g : x_g < x_f} and holds
+// m = #{g : x_g == x_f} frames, so its score is the average of zt[r .. r+m)
+// summed in rank order, as in the sorted form.  Grid (frame blocks,
+// components); the component's values pass through shared memory in tiles.
+constexpr int kCopulaTile = 4096;
+
+__global__ void __launch_bounds__(256) copula_count_kernel(const double* __restrict__ XF, int natoms, int T,
+                                                           const double* __restrict__ zt, double* __restrict__ Z)
+{
+    __shared__ double tile[kCopulaTile];
+    const int    nc   = natoms * 3, comp = blockIdx.y;
+    const int    f    = blockIdx.x * blockDim.x + threadIdx.x;
+    const double v    = f < T ? XF[(size_t)f * nc + comp] : 0.0;
+    int          lt = 0, eq = 0;
+    for (int t0 = 0; t0 < T; t0 += kCopulaTile)
+    {
+        const int n = min(kCopulaTile, T - t0);
+        __syncthreads(); // the previous tile is consumed
+        for (int e = threadIdx.x; e < n; e += blockDim.x)
+            tile[e] = XF[(size_t)(t0 + e) * nc + comp];
+        __syncthreads();
+        for (int e = 0; e < n; ++e)
+        {
+            const double u = tile[e];
+            lt += u < v;
+            eq += u == v;
+        }
+    }
+    if (f >= T)
+        return;
+    double avg = 0.0;
+    for (int t = lt; t < lt + eq; ++t)
+        avg = __dadd_rn(avg, zt[t]);
+    Z[(size_t)f * nc + comp] = __ddiv_rn(avg, (double)eq);
 }
 
 // Block b = hi*(hi+1)/2 + lo (lo <= hi): 9 co-moments summed over frames in order.
@@ -314,6 +354,12 @@ void launch_frame_major(const double* xyz, int natoms, int T, double* XF, int* s
 void launch_copula(const double* XF, int natoms, int T, double* zt, double* Z, cudaStream_t s)
 {
     probit_table_kernel<<<(T + 127) / 128, 128, 0, s>>>(T, zt);
+    if (T > kCopulaSortMax)
+    {
+        copula_count_kernel<<<dim3((unsigned)((T + 255) / 256), (unsigned)(natoms * 3)), 256, 0, s>>>(XF, natoms, T,
+                                                                                                     zt, Z);
+        return;
+    }
     int P = 1;
     while (P < T)
         P <<= 1;

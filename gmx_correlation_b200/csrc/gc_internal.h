@@ -8,6 +8,9 @@
 
 namespace gc {
 
+// Largest frame count the C ABI accepts (32-bit count and index arithmetic).
+constexpr int kMaxFrames = 1 << 24;
+
 // Device status bits raised by kernels (checked by the host after a run).
 enum : int
 {
@@ -30,14 +33,16 @@ void launch_ksg_prepare(const double* xyz, int natoms, int T, double* X, int* st
 void launch_ksg_check_rows(const double* X, long n, int* status, cudaStream_t s);
 
 // Exact FP64 brute-force KSG statistics for pairs [pair_begin, pair_begin+pair_count):
-// writes cnt[i * pair_count + pl] = n_x | n_y << 16 for every query frame i.
+// writes cnt[pl * T + i] = n_x | n_y << 16 for every query frame i, or with
+// cnt_y (wide counts, any frame count) cnt[pl * T + i] = n_x and
+// cnt_y[pl * T + i] = n_y.
 // pair_ab (optional): device (a1, a2) per local pair index of an explicit list.
 void launch_ksg_exact(const double* X, int T, int K, long pair_begin, long pair_count, uint32_t* cnt,
-                      cudaStream_t s, const int2* pair_ab = nullptr);
+                      cudaStream_t s, const int2* pair_ab = nullptr, uint32_t* cnt_y = nullptr);
 
 // MI per pair from the per-query counts, summed in frame order as mir_xnyn does.
 void launch_ksg_finalize(const uint32_t* cnt, long pair_count, int T, int K, const double* psi,
-                         double* pair_mi, cudaStream_t s);
+                         double* pair_mi, cudaStream_t s, const uint32_t* cnt_y = nullptr);
 
 // ---- Transfer entropy ------------------------------------------------------
 // xyz [natoms][T][3] -> XT [3*natoms][T] (component-major copy, raw values),
@@ -45,8 +50,10 @@ void launch_ksg_finalize(const uint32_t* cnt, long pair_count, int T, int K, con
 void launch_transpose_components(const double* xyz, int natoms, int T, double* XT, int* status,
                                  cudaStream_t s);
 // Exact FP64 TE statistics for every ordered pair; cnt[qi * npairs + q] =
-// {n_xp | n_xfxp << 16, n_ypxp}.
-void launch_te_exact(const double* XT, int natoms, int T, int K, int lag, uint2* cnt, cudaStream_t s);
+// {n_xp | n_xfxp << 16, n_ypxp}, or with wide (any frame count) {n_xp,
+// n_xfxp} there and {n_ypxp, 0} at cnt[(Nv + qi) * npairs + q].
+void launch_te_exact(const double* XT, int natoms, int T, int K, int lag, uint2* cnt, cudaStream_t s,
+                     bool wide = false);
 // FP32 copy of the raw coordinates and per-atom error bounds for launch_te_fast.
 void launch_te_x32(const double* XT, int natoms, int T, float4* X32, float* eps_atom, cudaStream_t s);
 // TE statistics from FP32 distances with exact FP64 repair (same counts as launch_te_exact).
@@ -54,7 +61,7 @@ void launch_te_fast(const double* XT, const float4* X32, const float* eps_atom, 
                     uint2* cnt, cudaStream_t s);
 // TE per ordered pair q = a1*(natoms-1) + (a2 < a1 ? a2 : a2-1), into te[a1*n+a2].
 void launch_te_finalize(const uint2* cnt, int natoms, int T, int K, int lag, const double* psi,
-                        double* te_mat, cudaStream_t s);
+                        double* te_mat, cudaStream_t s, bool wide = false);
 
 // ---- Gaussian and copula MI ------------------------------------------------
 // xyz [natoms][T][3] -> XF [T][3*natoms] (frame-major), status on non-finite.

@@ -136,7 +136,8 @@ constexpr int kExactQBlock = 64;
 
 __global__ void __launch_bounds__(kExactWarps * 32)
     ksg_exact_kernel(const double* __restrict__ X, int T, int K, long pair_begin, long pair_count,
-                     const int2* __restrict__ pair_ab, int nqb, int rank_shift, uint32_t* __restrict__ cnt)
+                     const int2* __restrict__ pair_ab, int nqb, int rank_shift, uint32_t* __restrict__ cnt,
+                     uint32_t* __restrict__ cnt_y)
 {
     __shared__ unsigned hist[kExactWarps][256];
     const int  warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -159,20 +160,40 @@ __global__ void __launch_bounds__(kExactWarps * 32)
 #pragma unroll 1
     for (int i = i0 + warp; i < i1; i += kExactWarps)
     {
-        const uint32_t c = exact_query(X, T, K, a1, a2, i, box, rank_shift, hist[warp], lane);
+        int nx, ny;
+        exact_query_nxy(X, T, K, a1, a2, i, box, rank_shift, hist[warp], lane, nx, ny);
         if (lane == 0)
-            cnt[(size_t)pl * T + i] = c;
+        {
+            if (cnt_y) // wide counts: n_x and n_y in separate planes
+            {
+                cnt[(size_t)pl * T + i]   = (uint32_t)nx;
+                cnt_y[(size_t)pl * T + i] = (uint32_t)ny;
+            }
+            else
+                cnt[(size_t)pl * T + i] = (uint32_t)nx | ((uint32_t)ny << 16);
+        }
     }
 }
 
 // MI = psi[N] + (psi[K] - 1/K) - (1/N) * sum_i (psi[n_x,i] + psi[n_y,i]),
 // summed over i in frame order (lib/kraskov.cpp:1262, :1303-1318).
-__global__ void ksg_finalize_kernel(const uint32_t* __restrict__ cnt, long pair_count, int T, int K,
-                                    const double* __restrict__ psi, double* __restrict__ pair_mi)
+// cnt_y != nullptr: wide counts (n_x in cnt, n_y in cnt_y, 32 bits each).
+__global__ void ksg_finalize_kernel(const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ cnt_y,
+                                    long pair_count, int T, int K, const double* __restrict__ psi,
+                                    double* __restrict__ pair_mi)
 {
     const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (p >= pair_count)
         return;
+    if (cnt_y)
+    {
+        double s = 0.0;
+        for (int i = 0; i < T; ++i)
+            s = __dadd_rn(s, __dadd_rn(psi[cnt[(size_t)p * T + i]], psi[cnt_y[(size_t)p * T + i]]));
+        const double phiK = __dsub_rn(psi[K], __ddiv_rn(1.0, (double)K));
+        pair_mi[p]        = __dsub_rn(__dadd_rn(psi[T], phiK), __ddiv_rn(s, (double)T));
+        return;
+    }
     // 16 frames' counts and digamma terms are fetched together; the sum
     // itself stays sequential in frame order
     double s = 0.0;
@@ -225,19 +246,19 @@ void launch_ksg_check_rows(const double* X, long n, int* status, cudaStream_t s)
 }
 
 void launch_ksg_exact(const double* X, int T, int K, long pair_begin, long pair_count, uint32_t* cnt,
-                      cudaStream_t s, const int2* pair_ab)
+                      cudaStream_t s, const int2* pair_ab, uint32_t* cnt_y)
 {
     const int  nqb   = (T + kExactQBlock - 1) / kExactQBlock;
     const long tasks = pair_count * nqb;
     const int  rank_shift = rank_top_shift(ksg_box_count(T, K), T);
     ksg_exact_kernel<<<(unsigned)tasks, kExactWarps * 32, 0, s>>>(X, T, K, pair_begin, pair_count, pair_ab, nqb,
-                                                                  rank_shift, cnt);
+                                                                  rank_shift, cnt, cnt_y);
 }
 
 void launch_ksg_finalize(const uint32_t* cnt, long pair_count, int T, int K, const double* psi,
-                         double* pair_mi, cudaStream_t s)
+                         double* pair_mi, cudaStream_t s, const uint32_t* cnt_y)
 {
-    ksg_finalize_kernel<<<(unsigned)((pair_count + 127) / 128), 128, 0, s>>>(cnt, pair_count, T, K, psi,
+    ksg_finalize_kernel<<<(unsigned)((pair_count + 127) / 128), 128, 0, s>>>(cnt, cnt_y, pair_count, T, K, psi,
                                                                             pair_mi);
 }
 

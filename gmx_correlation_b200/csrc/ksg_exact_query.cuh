@@ -7,11 +7,12 @@
 
 namespace gc {
 
-// Returns n_x | n_y << 16 for query frame i of pair (a1, a2), x = a1.
-// X: [3*natoms][T] normalised rows; hist: 256 words of this warp's
-// shared memory.  All lanes return the same value.
-__device__ __forceinline__ uint32_t exact_query(const double* __restrict__ X, int T, int K, int a1, int a2,
-                                                int i, int box, int rank_shift, unsigned* hist, int lane)
+// n_x and n_y of query frame i of pair (a1, a2), x = a1.  X: [3*natoms][T]
+// normalised rows; hist: 256 words of this warp's shared memory.  All lanes
+// get the same values.
+__device__ __forceinline__ void exact_query_nxy(const double* __restrict__ X, int T, int K, int a1, int a2, int i,
+                                                int box, int rank_shift, unsigned* hist, int lane, int& nx_out,
+                                                int& ny_out)
 {
     const double* __restrict__ ra0 = X + (size_t)(a1 * 3 + 0) * T;
     const double* __restrict__ ra1 = X + (size_t)(a1 * 3 + 1) * T;
@@ -98,8 +99,16 @@ __device__ __forceinline__ uint32_t exact_query(const double* __restrict__ X, in
         nx += dx <= ex;
         ny += dy <= ey;
     }
-    nx = __reduce_add_sync(kFull, nx);
-    ny = __reduce_add_sync(kFull, ny);
+    nx_out = __reduce_add_sync(kFull, nx);
+    ny_out = __reduce_add_sync(kFull, ny);
+}
+
+// The same counts packed as n_x | n_y << 16 (nframes <= 65535).
+__device__ __forceinline__ uint32_t exact_query(const double* __restrict__ X, int T, int K, int a1, int a2, int i,
+                                                int box, int rank_shift, unsigned* hist, int lane)
+{
+    int nx, ny;
+    exact_query_nxy(X, T, K, a1, a2, i, box, rank_shift, hist, lane, nx, ny);
     return (uint32_t)nx | ((uint32_t)ny << 16);
 }
 

@@ -38,7 +38,7 @@ constexpr int kTeQBlock = 64;
 
 __global__ void __launch_bounds__(kTeWarps * 32)
     te_exact_kernel(const double* __restrict__ XT, int natoms, int T, int K, int lag, int nqb,
-                    uint2* __restrict__ cnt)
+                    uint2* __restrict__ cnt, bool wide)
 {
     __shared__ unsigned hist[kTeWarps][256];
     const int  warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -55,9 +55,18 @@ __global__ void __launch_bounds__(kTeWarps * 32)
 #pragma unroll 1
     for (int qi = i0 + warp; qi < i1; qi += kTeWarps)
     {
-        const uint2 c = te_exact_query(XT, T, K, lag, a1, a2, qi, hist[warp], lane);
+        int xp, xf, yp;
+        te_exact_query_n(XT, T, K, lag, a1, a2, qi, hist[warp], lane, xp, xf, yp);
         if (lane == 0)
-            cnt[(size_t)qi * npairs + q] = c;
+        {
+            if (wide)
+            {
+                cnt[(size_t)qi * npairs + q]        = make_uint2((unsigned)xp, (unsigned)xf);
+                cnt[(size_t)(Nv + qi) * npairs + q] = make_uint2((unsigned)yp, 0u);
+            }
+            else
+                cnt[(size_t)qi * npairs + q] = make_uint2((unsigned)xp | ((unsigned)xf << 16), (unsigned)yp);
+        }
     }
 }
 
@@ -261,7 +270,7 @@ __global__ void __launch_bounds__(kTeWarps * 32)
 // te_sum += psi_k + psi[n_xp+1] - psi[n_xfxp+1] - psi[n_ypxp+1] over qi in
 // order, then te_sum / N_valid (lib/transfer_entropy.cpp:195-204).
 __global__ void te_finalize_kernel(const uint2* __restrict__ cnt, int natoms, int T, int K, int lag,
-                                   const double* __restrict__ psi, double* __restrict__ te_mat)
+                                   const double* __restrict__ psi, double* __restrict__ te_mat, bool wide)
 {
     const long npairs = (long)natoms * (natoms - 1);
     const long q      = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -272,6 +281,14 @@ __global__ void te_finalize_kernel(const uint2* __restrict__ cnt, int natoms, in
     for (int qi = 0; qi < Nv; ++qi)
     {
         const uint2 c   = cnt[(size_t)qi * npairs + q];
+        if (wide)
+        {
+            const int    xp = min((int)c.x, Nv), xf = min((int)c.y, Nv);
+            const int    yp = min((int)cnt[(size_t)(Nv + qi) * npairs + q].x, Nv);
+            const double t  = __dsub_rn(__dsub_rn(__dadd_rn(psi[K], psi[xp + 1]), psi[xf + 1]), psi[yp + 1]);
+            sum             = __dadd_rn(sum, t);
+            continue;
+        }
         const int   xp  = min((int)(c.x & 0xFFFFu), Nv);
         const int   xf  = min((int)(c.x >> 16), Nv);
         const int   yp  = min((int)c.y, Nv);
@@ -289,12 +306,12 @@ void launch_transpose_components(const double* xyz, int natoms, int T, double* X
     transpose_components_kernel<<<1184, 256, 0, s>>>(xyz, natoms, T, XT, status);
 }
 
-void launch_te_exact(const double* XT, int natoms, int T, int K, int lag, uint2* cnt, cudaStream_t s)
+void launch_te_exact(const double* XT, int natoms, int T, int K, int lag, uint2* cnt, cudaStream_t s, bool wide)
 {
     const int  Nv     = T - lag;
     const int  nqb    = (Nv + kTeQBlock - 1) / kTeQBlock;
     const long npairs = (long)natoms * (natoms - 1);
-    te_exact_kernel<<<(unsigned)(npairs * nqb), kTeWarps * 32, 0, s>>>(XT, natoms, T, K, lag, nqb, cnt);
+    te_exact_kernel<<<(unsigned)(npairs * nqb), kTeWarps * 32, 0, s>>>(XT, natoms, T, K, lag, nqb, cnt, wide);
 }
 
 void launch_te_x32(const double* XT, int natoms, int T, float4* X32, float* eps_atom, cudaStream_t s)
@@ -312,10 +329,10 @@ void launch_te_fast(const double* XT, const float4* X32, const float* eps_atom, 
 }
 
 void launch_te_finalize(const uint2* cnt, int natoms, int T, int K, int lag, const double* psi, double* te_mat,
-                        cudaStream_t s)
+                        cudaStream_t s, bool wide)
 {
     const long npairs = (long)natoms * (natoms - 1);
-    te_finalize_kernel<<<(unsigned)((npairs + 127) / 128), 128, 0, s>>>(cnt, natoms, T, K, lag, psi, te_mat);
+    te_finalize_kernel<<<(unsigned)((npairs + 127) / 128), 128, 0, s>>>(cnt, natoms, T, K, lag, psi, te_mat, wide);
 }
 
 } // namespace gc

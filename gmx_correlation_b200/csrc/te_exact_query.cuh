@@ -13,8 +13,8 @@ namespace gc {
 // selection; only its value matters, so no tie rule); the counts are strict
 // (< eps).  Returns (n_xp | n_xfxp << 16, n_ypxp) on every lane.  hist: 256
 // words of this warp's shared memory.
-__device__ __forceinline__ uint2 te_exact_query(const double* __restrict__ XT, int T, int K, int lag, int a1, int a2,
-                                                int qi, unsigned* hist, int lane)
+__device__ __forceinline__ void te_exact_query_n(const double* __restrict__ XT, int T, int K, int lag, int a1, int a2,
+                                                 int qi, unsigned* hist, int lane, int& n_xp, int& n_xfxp, int& n_ypxp)
 {
     const double* __restrict__ A0 = XT + (size_t)(a1 * 3 + 0) * T;
     const double* __restrict__ A1 = XT + (size_t)(a1 * 3 + 1) * T;
@@ -52,10 +52,18 @@ __device__ __forceinline__ uint2 te_exact_query(const double* __restrict__ XT, i
         nypxp += fmax(b, c) < eps;
         nxp += b < eps;
     }
-    nxfxp = __reduce_add_sync(kFull, nxfxp);
-    nypxp = __reduce_add_sync(kFull, nypxp);
-    nxp   = __reduce_add_sync(kFull, nxp);
-    return make_uint2((unsigned)nxp | ((unsigned)nxfxp << 16), (unsigned)nypxp);
+    n_xfxp = __reduce_add_sync(kFull, nxfxp);
+    n_ypxp = __reduce_add_sync(kFull, nypxp);
+    n_xp   = __reduce_add_sync(kFull, nxp);
+}
+
+// The same counts packed as (n_xp | n_xfxp << 16, n_ypxp) (N_valid <= 65535).
+__device__ __forceinline__ uint2 te_exact_query(const double* __restrict__ XT, int T, int K, int lag, int a1, int a2,
+                                                int qi, unsigned* hist, int lane)
+{
+    int xp, xf, yp;
+    te_exact_query_n(XT, T, K, lag, a1, a2, qi, hist, lane, xp, xf, yp);
+    return make_uint2((unsigned)xp | ((unsigned)xf << 16), (unsigned)yp);
 }
 
 } // namespace gc

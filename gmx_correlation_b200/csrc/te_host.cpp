@@ -35,8 +35,8 @@ gc_status te_validate(int natoms, int T, int k, int lag)
         return fail(GC_ERR_INVALID, "te_matrix: lag must be non-negative");
     if (natoms < 0 || T < 0)
         return fail(GC_ERR_INVALID, "te_matrix: negative trajectory size");
-    if (T > 65535)
-        return fail(GC_ERR_INVALID, "te_matrix: this build supports at most 65535 frames");
+    if (T > gc::kMaxFrames)
+        return fail(GC_ERR_INVALID, "te_matrix: this build supports at most 16777216 frames");
     return GC_OK;
 }
 
@@ -256,6 +256,7 @@ struct gc_te_plan
     int                 natoms = 0, T = 0, K = 0, lag = 0, Nv = 0, path = GC_PATH_AUTO;
     long                npairs = 0; // ordered pairs
     bool                walk   = false;
+    bool                wide   = false; // counts above 16 bits (exact kernel, two planes)
     cudaStream_t        stream = nullptr;
     cudaEvent_t         ev0 = nullptr, ev1 = nullptr, ev_done = nullptr;
     gc::host::TeTraj    tt;
@@ -289,6 +290,11 @@ gc_status gc_te_plan_create(int natoms, int nframes, int k, int lag, const gc_op
     p->path   = o.path;
     p->npairs = (long)natoms * (natoms - 1);
     p->walk   = o.path != GC_PATH_EXACT_FP64 && p->Nv - 1 <= 16384;
+    // more than 65535 valid frames: 32-bit counts, which only the exact
+    // kernel writes (the walk stops at 16385 frames anyway)
+    p->wide = p->Nv > 65535;
+    if (p->wide)
+        p->path = GC_PATH_EXACT_FP64;
     GC_TRY_CUDA(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, p->device));
     GC_TRY_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
     GC_TRY_CUDA(cudaEventCreate(&p->ev0));
@@ -305,6 +311,8 @@ gc_status gc_te_plan_create(int natoms, int nframes, int k, int lag, const gc_op
         Q = ksg_block_queries(2 * natoms, p->Nv, 16.0 * (1 << 30), 32 * warps);
     }
     GC_TRY(p->tt.create(natoms, nframes, k, lag, Q));
+    if (p->wide) // (n_xp, n_xfxp) then (n_ypxp, 0): two planes
+        GC_TRY(p->tt.cnt.alloc((size_t)2 * p->Nv * p->npairs));
     if (p->walk)
     {
         std::vector<std::vector<gc::TeParams>> waves;
@@ -339,11 +347,11 @@ gc_status gc_te_plan_run(gc_te_plan* p, const double* d_xyz, double* d_te, void*
     else
     {
         if (p->path == GC_PATH_EXACT_FP64)
-            gc::launch_te_exact(p->tt.XT.p, n, p->T, p->K, p->lag, p->tt.cnt.p, s);
+            gc::launch_te_exact(p->tt.XT.p, n, p->T, p->K, p->lag, p->tt.cnt.p, s, p->wide);
         else
             gc::launch_te_fast(p->tt.XT.p, p->tt.X32.p, p->tt.eps.p, n, p->T, p->K, p->lag, p->tt.cnt.p, s);
         GC_TRY_CUDA(cudaEventRecord(p->ev1, s));
-        gc::launch_te_finalize(p->tt.cnt.p, n, p->T, p->K, p->lag, p->tt.psi.p, d_te, s);
+        gc::launch_te_finalize(p->tt.cnt.p, n, p->T, p->K, p->lag, p->tt.psi.p, d_te, s, p->wide);
         p->launches += 2;
     }
     GC_TRY_CUDA(cudaGetLastError());
@@ -413,14 +421,22 @@ gc_status gc_te_plan_counts(gc_te_plan* p, int a1, int a2, int32_t* n_xp, int32_
     else // query-major [qi][npairs]
         GC_TRY_CUDA(cudaMemcpy2D(c.data(), sizeof(uint2), p->tt.cnt.p + q, sizeof(uint2) * p->npairs,
                                  sizeof(uint2), (size_t)p->Nv, cudaMemcpyDeviceToHost));
+    std::vector<uint2> c2;
+    if (p->wide) // the n_ypxp plane
+    {
+        c2.resize((size_t)p->Nv);
+        GC_TRY_CUDA(cudaMemcpy2D(c2.data(), sizeof(uint2), p->tt.cnt.p + (size_t)p->Nv * p->npairs + q,
+                                 sizeof(uint2) * p->npairs, sizeof(uint2), (size_t)p->Nv, cudaMemcpyDeviceToHost));
+    }
     for (int i = 0; i < p->Nv; ++i)
     {
+        const uint2 v = c[(size_t)i];
         if (n_xp)
-            n_xp[i] = (int32_t)(c[(size_t)i].x & 0xFFFFu);
+            n_xp[i] = (int32_t)(p->wide ? v.x : (v.x & 0xFFFFu));
         if (n_xfxp)
-            n_xfxp[i] = (int32_t)(c[(size_t)i].x >> 16);
+            n_xfxp[i] = (int32_t)(p->wide ? v.y : (v.x >> 16));
         if (n_ypxp)
-            n_ypxp[i] = (int32_t)c[(size_t)i].y;
+            n_ypxp[i] = (int32_t)(p->wide ? c2[(size_t)i].x : v.y);
     }
     return GC_OK;
 }

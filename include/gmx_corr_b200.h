@@ -160,7 +160,7 @@ gc_status gc_te_batch(const gc_traj_view* trajs, const int* ks, int ntraj, int l
                       double* const* te);
 void      gc_te_batch_release(void);
 
-/* Gaussian-copula MI matrices of ntraj trajectories (nframes <= 16384 each)
+/* Gaussian-copula MI matrices of ntraj trajectories
  * in one captured CUDA graph, with the conventions of gc_gcmi_matrix.  The
  * last batch's workspace and graph are kept for a repeated call with the
  * same shapes; gc_gcmi_batch_release frees them.  No counterpart in the

@@ -107,3 +107,28 @@ def test_te_walk_counts_equal_oracle(gc, oracle):
         np.testing.assert_array_equal(nyp, d["nypxp"])
         assert d_te[a1, a2].item() == d["te"]
     plan.close()
+
+
+def test_gcmi_beyond_the_shared_memory_sort(gc, oracle):
+    """More than 16384 frames: the copula scores come from rank counting
+    instead of the shared-memory sort, with the reference's midranks (ties
+    from 0.01 nm rounding)."""
+    from gmx_correlation_b200.synth import synth_traj
+    x = np.round(synth_traj(4, 17000, 3, 0.08, seed=5) / 0.01) * 0.01
+    np.testing.assert_allclose(gc.gcmi_corrmatrix(x), oracle.gcmi_matrix(x), rtol=1e-11, atol=1e-13)
+
+
+def test_more_than_65535_frames(gc):
+    """Counts above 16 bits (the exact kernels' two-plane layout): KSG of a
+    65,600-frame pair against the reference itself (oracle/_ref), and the
+    per-query counts against the reference's own neighbour search."""
+    from oracle import Reference
+    from gmx_correlation_b200.synth import synth_traj
+    ref = Reference()
+    x = synth_traj(2, 65600, 2, 0.08, seed=9, fp32=True)
+    mat, nx, ny = gc.kraskov_corrmatrix(x, 4, detail=True)
+    np.testing.assert_array_equal(mat, ref.ksg_matrix(x, 4))
+    d = ref.ksg_pair_detail(x, 4, 1, 0)
+    np.testing.assert_array_equal(nx[0], d["nx"])
+    np.testing.assert_array_equal(ny[0], d["ny"])
+    assert nx.max() > 0 and mat[1, 0] == d["mi"]

@@ -25,8 +25,11 @@ inline gc_status fail(gc_status st, const std::string& msg)
     {                                                                                                \
         cudaError_t e_ = (call);                                                                     \
         if (e_ != cudaSuccess)                                                                       \
+        {                                                                                            \
+            cudaGetLastError(); /* a non-sticky error must not resurface in the next call */         \
             return fail(e_ == cudaErrorMemoryAllocation ? GC_ERR_OUT_OF_MEMORY : GC_ERR_CUDA,         \
                         std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+        }                                                                                            \
     } while (0)
 
 #define GC_TRY(expr)                                                                                 \

@@ -239,7 +239,23 @@ WalkConfig walk_config(int maxT, int k)
         std::lock_guard<std::mutex> lock(g_cfg_mutex);
         const auto                  it = g_cfg.find({maxT / 256, k});
         if (it != g_cfg.end())
-            return it->second;
+        {
+            // tuned on trajectories of up to 255 fewer frames: the staged rows
+            // of maxT frames may leave room for fewer warps
+            WalkConfig c = it->second;
+            if (c.staged)
+            {
+                const int w = walk_max_staged_warps(maxT);
+                if (w > 0)
+                    c.walk_warps = std::min(c.walk_warps, w);
+                else
+                {
+                    c.staged     = false;
+                    c.walk_warps = kWalkWarps;
+                }
+            }
+            return c;
+        }
     }
     WalkConfig c;
     walk_shape(maxT, &c.walk_warps, &c.staged);

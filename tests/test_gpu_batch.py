@@ -97,3 +97,16 @@ def test_te_batch_short_trajectory_is_zero(gc):
     assert not outs[0].any()
     np.testing.assert_array_equal(outs[1], gc.te_matrix(xs[1], 10, 3))
     gc.batch_release()
+
+
+def test_tuned_walk_shape_fits_longer_rows_of_its_class(gc):
+    """The autotuner remembers a walk shape per (frames / 256, k); a later
+    trajectory of the same class with more frames (4000 after 3840) gets the
+    shape clamped to what its staged rows leave room for."""
+    from gmx_correlation_b200.synth import synth_traj
+    gc.ksg_batch([synth_traj(12, 3840, 4, 0.08, 3, fp32=True)], [100])
+    gc.batch_release()
+    x = synth_traj(6, 4000, 4, 0.08, 4, fp32=True)
+    np.testing.assert_array_equal(gc.kraskov_corrmatrix(x, 100),
+                                  gc.kraskov_corrmatrix(x, 100, path=gc.PATH_EXACT_FP64))
+    gc.release_cache()

@@ -36,6 +36,12 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", f"-I{INCLUDE}", f"-I{CSRC}",
              f"-I{CSRC / 'dropin'}", f"-I{CUDA_HOME / 'include'}"]
 
+# Extra preprocessor definitions for both compilers (build-time settings of
+# the kernels, e.g. GC_EXTRA_DEFS="-DGC_BAND_CAP=16"); empty for the product.
+EXTRA_DEFS = os.environ.get("GC_EXTRA_DEFS", "").split()
+NVCC_FLAGS += EXTRA_DEFS
+CXX_FLAGS += EXTRA_DEFS
+
 CU_SOURCES = sorted(CSRC.glob("*.cu"))
 CPP_SOURCES = sorted(CSRC.glob("*.cpp")) + sorted((CSRC / "dropin").glob("*.cpp"))
 HEADERS = (sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))

@@ -314,6 +314,153 @@ __device__ __forceinline__ unsigned long long pack_walk(int bstar, int prefix, i
 
 } // namespace
 
+// One query group of a walk task (pass 1 below): lane iq = g * 32 + lane
+// walks the sorted row of its query and histograms v = max(s, d), d the other
+// marginal's FP32 distance to the entry's frame, dist_other(frame).  Writes
+// the lane's walk result; clears and uses this warp's histogram at base.
+template <bool LO, class DistFn>
+__device__ __forceinline__ void walk_query_group(const WalkParams& p, long pl, int iq, bool live, const LaneSetup& u,
+                                                 DistFn&& dist_other, unsigned char* base, int lane)
+{
+    const int          K = p.K, Llen = p.T - 1, shift = p.shift;
+    uint8_t*           hist = base + lane * 4;
+    auto               H    = [hist](unsigned b) -> uint8_t& { return hist[(b >> 2) * 128 + (b & 3)]; };
+    constexpr unsigned kTop = kWalkBuckets - 1; // open-ended index above the range, never read
+    const float        inf  = __int_as_float(0x7f800000);
+    {
+        uint4* h4 = reinterpret_cast<uint4*>(base);
+        for (int e = lane; e < kWalkBuckets * 32 / 16; e += 32)
+            h4[e] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    __syncwarp();
+
+    // Histogram index of v: LO: 0 for v < L, then buckets of 2^shift
+    // float ulps from L; otherwise buckets from L (v < L counted in
+    // cnt_lo).  Index b starts at value bits Lh + (b << shift) (b >= 1
+    // when LO); the last index takes everything above the range.
+    const unsigned Lh   = LO ? u.Lb - (1u << shift) : u.Lb;
+    auto           hidx = [Lh, shift](float v) -> unsigned {
+        if (LO)
+            return (unsigned)min(max((int)(__float_as_uint(v) - Lh) >> shift, 0), (int)kTop);
+        return min((__float_as_uint(v) - Lh) >> shift, kTop);
+    };
+    // Every 16 entries the indices below the current value are final
+    // (later entries have v >= s), so their running sum R decides the stop
+    // value.  The rows end in NaN up to a 4-entry boundary, which the
+    // take test (s <= stop) never passes, so taken entries form a prefix
+    // of each group and a group short of 4 ends the walk.
+    const float4* Sg = reinterpret_cast<const float4*>(u.rw.S); // 4-entry groups of this lane's row
+    const uint2*  Pg = reinterpret_cast<const uint2*>(u.rw.P);
+    const size_t  gs = (size_t)p.Qp;                            // group stride
+    int           m_end = 0, cnt_lo = 0, R = 0, thr = 0, grp = 0;
+    unsigned      wrap = 0u; // bit 8 set once a counter below the top passed 255
+    float         stop = inf;
+    bool          walking = live;
+    float4        s4      = make_float4(inf, inf, inf, inf);
+    uint2         j4      = make_uint2(0u, 0u);
+    if (live)
+    {
+        s4 = Sg[0];
+        j4 = Pg[0];
+    }
+    const int last = (Llen - 1) >> 2; // the last (possibly partial) group
+    while (walking)
+    {
+        if (grp > last) // the whole row walked
+        {
+            m_end = Llen;
+            break;
+        }
+        // prefetch the next group (the last group again at the end)
+        const int      nxt   = grp < last ? grp + 1 : grp;
+        const float4   ns4   = Sg[(size_t)nxt * gs];
+        const uint2    nj4   = Pg[(size_t)nxt * gs];
+        const float    sv[4] = {s4.x, s4.y, s4.z, s4.w};
+        const unsigned jv[4] = {j4.x & 0xFFFFu, j4.x >> 16, j4.y & 0xFFFFu, j4.y >> 16};
+        bool           tkn[4];
+        // Branch-free: every slot gathers and adds 0 or 1 to its counter.
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+        {
+            tkn[q]          = sv[q] <= stop;
+            const float v   = fmaxf(sv[q], dist_other(jv[q]));
+            bool        inc = tkn[q];
+            if (!LO)
+            {
+                const bool below = v < u.L;
+                cnt_lo += inc && below;
+                inc = inc && !below;
+            }
+            uint8_t&       c  = H(hidx(v));
+            const unsigned h1 = (unsigned)c + (inc ? 1u : 0u);
+            c                 = (uint8_t)h1;
+            wrap |= h1;
+        }
+        ++grp;
+        if (!tkn[3])
+        {
+            walking = false;
+            m_end   = (grp - 1) * 4 + (int)tkn[0] + (int)tkn[1] + (int)tkn[2];
+        }
+        else if ((grp & 3) == 0)
+        {
+            H(kTop) = 0; // at most 16 increments between clears: never wraps
+            if (stop == inf)
+            {
+                const float sl = sv[3];
+                const int   bn = (LO || sl >= u.L) ? (int)hidx(sl) : 0;
+                for (int b = thr; b < bn; ++b)
+                    R += H(b);
+                thr = max(thr, bn);
+                if (cnt_lo + R >= K)
+                    stop = __fadd_ru(__uint_as_float(Lh + ((unsigned)bn << shift)), u.e2);
+            }
+        }
+        s4 = ns4;
+        j4 = nj4;
+    }
+
+    // histogram index of the k-th value
+    if (live)
+    {
+        int bstar, prefix;
+        if (stop != inf)
+        {
+            // cum = #{v below index b + 1} >= K; step down while still >= K
+            int cum = cnt_lo + R, b = thr - 1;
+            while (b > 0 && cum - (int)H(b) >= K)
+            {
+                cum -= H(b);
+                --b;
+            }
+            bstar  = b;
+            prefix = cum - H(b);
+        }
+        else
+        {
+            int cum = cnt_lo, b = 0;
+            while (b < (int)kTop && cum + (int)H(b) < K)
+            {
+                cum += H(b);
+                ++b;
+            }
+            bstar  = b;
+            prefix = cum;
+        }
+        // index 0 under LO holds fewer than k entries, so the k-th value
+        // lies above it unless the input is not finite
+        const int reason = (wrap > 255u || (LO && bstar == 0)) ? kReasonBand
+                           : (bstar >= (int)kTop ? kReasonRange : 0);
+        // the result names buckets from L (index - 1 under LO)
+        p.wres[(size_t)pl * p.Q + iq] = pack_walk(LO ? bstar - 1 : bstar, prefix, m_end, reason);
+    }
+    if (p.walk_elems)
+    {
+        const unsigned we = __reduce_add_sync(kFull, live ? (unsigned)m_end : 0u);
+        if (lane == 0 && we)
+            atomicAdd(p.walk_elems, (unsigned long long)we);
+    }}
+
 // Pass 1: walk the sorted row, histogram v = max(s, d) per lane.  STAGED:
 // the pair's coordinate rows are copied into shared memory per task.  LO
 // (every k of the launch below 256): entries below the lower bound L count
@@ -329,21 +476,17 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
     __shared__ int       s_desc, s_next;
     const int            warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float4*              sx   = reinterpret_cast<float4*>(smem_raw);
+    // this warp's histogram: index b of a lane is byte b % 4 of word
+    // (b / 4) * 32 + lane, so the 32 lanes of a warp always hit 32 different banks
     unsigned char*       base = smem_raw + (STAGED ? (size_t)2 * B.maxT * 16 : 0) + (size_t)warp * kWalkBuckets * 32;
-    // histogram index b of this lane: byte b % 4 of word (b / 4) * 32 + lane,
-    // so the 32 lanes of a warp always hit 32 different banks
-    uint8_t* hist = base + lane * 4;
-    auto     H    = [hist](unsigned b) -> uint8_t& { return hist[(b >> 2) * 128 + (b & 3)]; };
-    constexpr unsigned kTop = kWalkBuckets - 1; // open-ended index above the range, never read
 
     const long long total = B.wprefix[B.n];
-    const float     inf   = __int_as_float(0x7f800000);
     Task            tk;
     int             dsc;
     while (next_task(B, total, &s_task, &s_desc, &s_next, tk, dsc))
     {
         const WalkParams& p       = B.d[dsc];
-        const int         T       = p.T, K = p.K, Llen = T - 1, shift = p.shift;
+        const int         T       = p.T;
         const int         ngroups = (p.Q + 31) >> 5;
         const float4* xa = p.X32 + (size_t)tk.a1 * T;
         const float4* xb = p.X32 + (size_t)tk.a2 * T;
@@ -377,142 +520,157 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
         // its unsorted distance row of this query
         const float4* X32o = STAGED ? (u.wx ? sx + T : sx) : u.X32o;
         const float*  Uo   = GU ? p.U + ((size_t)u.o * p.Qp + iql) * p.Tpad : nullptr;
-        {
-            uint4* h4 = reinterpret_cast<uint4*>(base);
-            for (int e = lane; e < kWalkBuckets * 32 / 16; e += 32)
-                h4[e] = make_uint4(0u, 0u, 0u, 0u);
-        }
-        __syncwarp();
-
-        // Histogram index of v: LO: 0 for v < L, then buckets of 2^shift
-        // float ulps from L; otherwise buckets from L (v < L counted in
-        // cnt_lo).  Index b starts at value bits Lh + (b << shift) (b >= 1
-        // when LO); the last index takes everything above the range.
-        const unsigned Lh   = LO ? u.Lb - (1u << shift) : u.Lb;
-        auto           hidx = [Lh, shift](float v) -> unsigned {
-            if (LO)
-                return (unsigned)min(max((int)(__float_as_uint(v) - Lh) >> shift, 0), (int)kTop);
-            return min((__float_as_uint(v) - Lh) >> shift, kTop);
-        };
-        // Every 16 entries the indices below the current value are final
-        // (later entries have v >= s), so their running sum R decides the stop
-        // value.  The rows end in NaN up to a 4-entry boundary, which the
-        // take test (s <= stop) never passes, so taken entries form a prefix
-        // of each group and a group short of 4 ends the walk.
-        const float4* Sg = reinterpret_cast<const float4*>(u.rw.S); // 4-entry groups of this lane's row
-        const uint2*  Pg = reinterpret_cast<const uint2*>(u.rw.P);
-        const size_t  gs = (size_t)p.Qp;                            // group stride
-        int           m_end = 0, cnt_lo = 0, R = 0, thr = 0, grp = 0;
-        unsigned      wrap = 0u; // bit 8 set once a counter below the top passed 255
-        float         stop = inf;
-        bool          walking = live;
-        float4        s4      = make_float4(inf, inf, inf, inf);
-        uint2         j4      = make_uint2(0u, 0u);
-        if (live)
-        {
-            s4 = Sg[0];
-            j4 = Pg[0];
-        }
-        const int last = (Llen - 1) >> 2; // the last (possibly partial) group
-        while (walking)
-        {
-            if (grp > last) // the whole row walked
-            {
-                m_end = Llen;
-                break;
-            }
-            // prefetch the next group (the last group again at the end)
-            const int      nxt   = grp < last ? grp + 1 : grp;
-            const float4   ns4   = Sg[(size_t)nxt * gs];
-            const uint2    nj4   = Pg[(size_t)nxt * gs];
-            const float    sv[4] = {s4.x, s4.y, s4.z, s4.w};
-            const unsigned jv[4] = {j4.x & 0xFFFFu, j4.x >> 16, j4.y & 0xFFFFu, j4.y >> 16};
-            bool           tkn[4];
-            // Branch-free: every slot gathers and adds 0 or 1 to its counter.
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-            {
-                tkn[q]          = sv[q] <= stop;
-                const float v   = fmaxf(sv[q], GU ? Uo[jv[q]] : dist3f(u.xo, X32o[jv[q]]));
-                bool        inc = tkn[q];
-                if (!LO)
-                {
-                    const bool below = v < u.L;
-                    cnt_lo += inc && below;
-                    inc = inc && !below;
-                }
-                uint8_t&       c  = H(hidx(v));
-                const unsigned h1 = (unsigned)c + (inc ? 1u : 0u);
-                c                 = (uint8_t)h1;
-                wrap |= h1;
-            }
-            ++grp;
-            if (!tkn[3])
-            {
-                walking = false;
-                m_end   = (grp - 1) * 4 + (int)tkn[0] + (int)tkn[1] + (int)tkn[2];
-            }
-            else if ((grp & 3) == 0)
-            {
-                H(kTop) = 0; // at most 16 increments between clears: never wraps
-                if (stop == inf)
-                {
-                    const float sl = sv[3];
-                    const int   bn = (LO || sl >= u.L) ? (int)hidx(sl) : 0;
-                    for (int b = thr; b < bn; ++b)
-                        R += H(b);
-                    thr = max(thr, bn);
-                    if (cnt_lo + R >= K)
-                        stop = __fadd_ru(__uint_as_float(Lh + ((unsigned)bn << shift)), u.e2);
-                }
-            }
-            s4 = ns4;
-            j4 = nj4;
-        }
-
-        // histogram index of the k-th value
-        if (live)
-        {
-            int bstar, prefix;
-            if (stop != inf)
-            {
-                // cum = #{v below index b + 1} >= K; step down while still >= K
-                int cum = cnt_lo + R, b = thr - 1;
-                while (b > 0 && cum - (int)H(b) >= K)
-                {
-                    cum -= H(b);
-                    --b;
-                }
-                bstar  = b;
-                prefix = cum - H(b);
-            }
-            else
-            {
-                int cum = cnt_lo, b = 0;
-                while (b < (int)kTop && cum + (int)H(b) < K)
-                {
-                    cum += H(b);
-                    ++b;
-                }
-                bstar  = b;
-                prefix = cum;
-            }
-            // index 0 under LO holds fewer than k entries, so the k-th value
-            // lies above it unless the input is not finite
-            const int reason = (wrap > 255u || (LO && bstar == 0)) ? kReasonBand
-                               : (bstar >= (int)kTop ? kReasonRange : 0);
-            // the result names buckets from L (index - 1 under LO)
-            p.wres[(size_t)tk.pl * p.Q + iq] = pack_walk(LO ? bstar - 1 : bstar, prefix, m_end, reason);
-        }
-        if (p.walk_elems)
-        {
-            const unsigned we = __reduce_add_sync(kFull, live ? (unsigned)m_end : 0u);
-            if (lane == 0 && we)
-                atomicAdd(p.walk_elems, (unsigned long long)we);
-        }
+        if (GU)
+            walk_query_group<LO>(p, tk.pl, iq, live, u, [&](unsigned j) { return Uo[j]; }, base, lane);
+        else
+            walk_query_group<LO>(p, tk.pl, iq, live, u, [&](unsigned j) { return dist3f(u.xo, X32o[j]); }, base,
+                                 lane);
         __syncwarp(); // the next group clears this warp's histogram
         }
         __syncthreads(); // every warp is done with the staged rows
+    }
+}
+
+// Pass 1, double-buffered: the CTA holds two walk tasks' coordinate rows in
+// shared memory, x and y as float2 and z apart (12 bytes a frame, so two
+// pairs and 32 warps' histograms fit), and warps move from a task to the
+// next without a CTA barrier: a warp that finds no query group left in task
+// i goes on to task i + 1 (the other buffer), and the last warp to leave
+// task i refills its buffer with task i + 2.  The distances are computed
+// with the same FP32 operations as dist3f, so the results equal the
+// single-buffered walk's.
+struct WalkSlot
+{
+    long long    t;      // global walk task, or -1: no more tasks
+    int          desc;   // descriptor of the task
+    int          next;   // query groups handed out
+    int          left;   // warps done with the task
+    volatile int gen;    // CTA-local index of the task this slot holds
+    Task         tk;
+};
+
+// Fills slot s with the next global walk task as CTA-local task `gen`: one
+// warp (lane 0 takes the task, all lanes copy the pair's rows).
+__device__ __forceinline__ void walk_slot_fill(const WalkBatch& B, WalkSlot& S, float2* xy, float* z, int gen,
+                                               int lane)
+{
+    long long t = 0;
+    int       d = 0;
+    if (lane == 0)
+    {
+        t = (long long)atomicAdd(B.counter, 1ull);
+        if (t < B.wprefix[B.n])
+            d = batch_desc(B.wprefix, B.n, t);
+        else
+            t = -1;
+    }
+    t = __shfl_sync(kFull, t, 0);
+    d = __shfl_sync(kFull, d, 0);
+    Task tk{};
+    if (t >= 0)
+    {
+        const WalkParams& p  = B.d[d];
+        const long long   lt = t - B.wprefix[d];
+        tk.c                 = (int)(lt / p.pair_count);
+        task_pair(p, (long)(lt - (long long)tk.c * p.pair_count), tk);
+        const int     T  = p.T;
+        const float4* xa = p.X32 + (size_t)tk.a1 * T;
+        const float4* xb = p.X32 + (size_t)tk.a2 * T;
+        for (int e = lane; e < T; e += 32)
+        {
+            const float4 va = xa[e], vb = xb[e];
+            xy[e]     = make_float2(va.x, va.y);
+            z[e]      = va.z;
+            xy[T + e] = make_float2(vb.x, vb.y);
+            z[T + e]  = vb.z;
+        }
+    }
+    __syncwarp();
+    if (lane == 0)
+    {
+        S.t    = t;
+        S.desc = d;
+        S.tk   = tk;
+        S.next = 0;
+        S.left = 0;
+        __threadfence_block(); // the rows and fields before the generation
+        S.gen = gen;
+    }
+    __syncwarp();
+}
+
+template <bool LO>
+__global__ void __launch_bounds__(1024, 1) ksg_walk_db_kernel(WalkBatch B)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ WalkSlot slot[2];
+    const int           warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const int           maxT = B.maxT;
+    // buffer b: xy [2 * maxT] float2 then z [2 * maxT] float (atom a1's rows, then a2's)
+    auto xyb = [&](int b) { return reinterpret_cast<float2*>(smem_raw + (size_t)b * 24 * maxT); };
+    auto zb  = [&](int b) { return reinterpret_cast<float*>(smem_raw + (size_t)b * 24 * maxT + (size_t)16 * maxT); };
+    unsigned char* base = smem_raw + (size_t)48 * maxT + (size_t)warp * kWalkBuckets * 32;
+    if (warp < 2)
+        walk_slot_fill(B, slot[warp], xyb(warp), zb(warp), warp, lane);
+    __syncthreads();
+    for (int i = 0;; ++i)
+    {
+        const int b  = i & 1;
+        WalkSlot& S  = slot[b];
+        // the slot holds task i once the warp that refilled it has published it;
+        // the wait is bounded (the refilling warp is resident and never waits)
+        int spins = 0;
+        while (S.gen != i)
+        {
+            if (++spins > (1 << 24))
+            {
+                if (lane == 0)
+                    atomicOr(B.d[0].status, kStatTimeout);
+                return;
+            }
+            __nanosleep(64);
+        }
+        __threadfence_block();
+        if (S.t < 0)
+            break;
+        const WalkParams& p       = B.d[S.desc];
+        const Task        tk      = S.tk;
+        const int         T       = p.T;
+        const int         ngroups = (p.Q + 31) >> 5;
+        const float2*     xy      = xyb(b);
+        const float*      z       = zb(b);
+        const float4*     ga      = p.X32 + (size_t)tk.a1 * T;
+        const float4*     gb      = p.X32 + (size_t)tk.a2 * T;
+        for (;;)
+        {
+            int gi = 0;
+            if (lane == 0)
+                gi = atomicAdd(&S.next, 1);
+            gi          = __shfl_sync(kFull, gi, 0);
+            const int g = tk.c * B.chunk + gi;
+            if (gi >= B.chunk || g >= ngroups)
+                break;
+            const int       iq   = g * 32 + lane;
+            const bool      live = iq < p.Q;
+            const int       iql  = live ? iq : 0;
+            const LaneSetup u    = lane_setup(p, tk.a1, tk.a2, iql, p.i0 + iql, ga, gb);
+            const float2*   oxy  = u.wx ? xy + T : xy;
+            const float*    oz   = u.wx ? z + T : z;
+            walk_query_group<LO>(
+                p, tk.pl, iq, live, u,
+                [&](unsigned j) {
+                    const float2 v = oxy[j];
+                    return fmaxf(fmaxf(fabsf(u.xo.x - v.x), fabsf(u.xo.y - v.y)), fabsf(u.xo.z - oz[j]));
+                },
+                base, lane);
+            __syncwarp(); // the next group clears this warp's histogram
+        }
+        int last = 0;
+        if (lane == 0)
+            last = atomicAdd(&S.left, 1) == nwarps - 1;
+        last = __shfl_sync(kFull, last, 0);
+        if (last) // every warp has left task i: its buffer takes task i + 2
+            walk_slot_fill(B, S, xyb(b), zb(b), i + 2, lane);
     }
 }
 
@@ -999,6 +1157,10 @@ cudaError_t launch_ksg_rows(const WalkBatch& b, long long rows, cudaStream_t s)
         kernel = ksg_rows_kernel<512, 8>;
     else if (threads == 512 && regs == 16)
         kernel = ksg_rows_kernel<512, 16>;
+#if GC_ROWS_128
+    else if (threads == 128 && regs == 16)
+        kernel = ksg_rows_kernel<128, 16>;
+#endif
     // static shared memory comes on top of the dynamic part: always raise
     // the limit to what this launch needs
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1022,6 +1184,15 @@ int walk_max_staged_warps(int maxT)
     return w >= 8 ? w : 0;
 }
 
+int walk_max_db_warps(int maxT)
+{
+    const size_t rows = (size_t)48 * maxT;
+    if (rows >= kSmemBudget)
+        return 0;
+    const int w = (int)((kSmemBudget - rows) / ((size_t)kWalkBuckets * 32));
+    return w > kWalkWarps ? kWalkWarps : w;
+}
+
 void walk_shape(int maxT, int* warps, bool* staged)
 {
     const int w = walk_max_staged_warps(maxT);
@@ -1029,9 +1200,20 @@ void walk_shape(int maxT, int* warps, bool* staged)
     *warps      = w > 0 ? w : kWalkWarps;
 }
 
-cudaError_t launch_ksg_walk(const WalkBatch& b, int warps, bool staged, int sms, cudaStream_t s, bool gather_u)
+cudaError_t launch_ksg_walk(const WalkBatch& b, int warps, bool staged, int sms, cudaStream_t s, bool gather_u,
+                            bool double_buffer)
 {
     const bool lo = b.maxK < 256;
+    if (double_buffer && !gather_u)
+    {
+        void (*kernel)(WalkBatch) = lo ? ksg_walk_db_kernel<true> : ksg_walk_db_kernel<false>;
+        const size_t smem = (size_t)48 * b.maxT + (size_t)warps * kWalkBuckets * 32;
+        cudaError_t  e    = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess)
+            return e;
+        kernel<<<sms, warps * 32, smem, s>>>(b);
+        return cudaGetLastError();
+    }
     staged        = staged && !gather_u;
     void (*kernel)(WalkBatch) =
         gather_u ? (lo ? ksg_walk_kernel<false, true, true> : ksg_walk_kernel<false, false, true>)

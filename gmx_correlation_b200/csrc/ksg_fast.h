@@ -9,7 +9,10 @@ namespace gc {
 constexpr int kWalkWarps   = 32;       // most warps per walk CTA
 constexpr int kFinishWarps = 16;       // warps per finish CTA
 constexpr int kWalkBuckets = 128;      // per-lane histogram buckets
-constexpr int kBandCap     = 20;       // band entries kept per lane
+#ifndef GC_BAND_CAP
+#define GC_BAND_CAP 20 // a build-time setting for timing other capacities
+#endif
+constexpr int kBandCap     = GC_BAND_CAP; // band entries kept per lane
 constexpr int kBandSlotBytes = 14;     // v, s, d (f32), row position in its range (u16)
 constexpr uint32_t kHandOver = 0xFFFFFFFFu; // cnt value of a query handed to the exact kernel
 
@@ -79,9 +82,12 @@ int walk_max_staged_warps(int maxT);
 // Each launcher returns the launch status (cudaGetLastError right after it).
 cudaError_t launch_ksg_x32(const double* X64, int natoms, int T, float4* X32, float* eps_atom, cudaStream_t s);
 cudaError_t launch_ksg_rows(const WalkBatch& b, long long rows, cudaStream_t s);
-// gather_u: the other marginal's distances come from the descriptors' U rows.
+// gather_u: the other marginal's distances come from the descriptors' U rows;
+// double_buffer: the double-buffered walk (two staged tasks per CTA).
 cudaError_t launch_ksg_walk(const WalkBatch& b, int warps, bool staged, int sms, cudaStream_t s,
-                            bool gather_u = false);
+                            bool gather_u = false, bool double_buffer = false);
+// Warps per CTA the double-buffered walk leaves room for (0: its rows do not fit).
+int walk_max_db_warps(int maxT);
 cudaError_t launch_ksg_finish(const WalkBatch& b, int sms, cudaStream_t s);
 // Exact FP64 statistics for every queued hand-over of the batch's
 // descriptors, then for any hand-over mark a queue could not hold (a scan of

@@ -20,6 +20,7 @@ struct WalkConfig
     int  pair_tile  = 16;
     int  chunk_mult = 4; // query groups per walk task = chunk_mult * walk_warps
     bool gather_u   = false; // other marginal from precomputed HBM rows (GC_VARIANT_HBM_GATHER)
+    bool double_buf = false; // the double-buffered walk kernel
 };
 
 // Fast-path workspace of one trajectory (all pairs, a shard, or a list): the

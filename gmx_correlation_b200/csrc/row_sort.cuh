@@ -306,6 +306,10 @@ __device__ __forceinline__ void sort_row(RowSortShared<THREADS>& sh, int N, int 
 // Shared memory of one sorted row of N entries: keys (N2 * 8 bytes) plus the
 // bucket counters and cursors; *threads and *regs pick the sort_row
 // instantiation (threads per row, distances per thread kept in registers).
+#ifndef GC_ROWS_128
+#define GC_ROWS_128 0 // a build-time setting: 128 threads x 16 distances for rows up to 2048 entries
+#endif
+
 inline size_t row_sort_smem(int N, int* threads, int* regs)
 {
     int N2 = 256;
@@ -315,8 +319,8 @@ inline size_t row_sort_smem(int N, int* threads, int* regs)
     // distances kept in registers, 8 per thread up to 2048 entries, then
     // 512 threads with 8 or 16 each (measured faster than 256 threads with
     // 16 or 32 at 4999 entries); longer rows recompute them
-    *threads = N <= 8 * 256 ? 256 : (N <= 16 * 512 ? 512 : 256);
-    *regs    = N <= 8 * 256 ? 8 : (N <= 8 * 512 ? 8 : (N <= 16 * 512 ? 16 : 0));
+    *threads = N <= 8 * 256 ? (GC_ROWS_128 ? 128 : 256) : (N <= 16 * 512 ? 512 : 256);
+    *regs    = N <= 8 * 256 ? (GC_ROWS_128 ? 16 : 8) : (N <= 8 * 512 ? 8 : (N <= 16 * 512 ? 16 : 0));
     return (size_t)N2 * 8 + (size_t)rows_skewed(nbin) * 8;
 }
 

@@ -922,6 +922,10 @@ cudaError_t launch_te_rows(const TeBatch& b, long long rows, cudaStream_t s)
         kernel = te_rows_kernel<512, 8>;
     else if (threads == 512 && regs == 16)
         kernel = te_rows_kernel<512, 16>;
+#if GC_ROWS_128
+    else if (threads == 128 && regs == 16)
+        kernel = te_rows_kernel<128, 16>;
+#endif
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;

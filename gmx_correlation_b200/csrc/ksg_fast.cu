@@ -536,7 +536,10 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_kernel(WalkBatch B)
 // pairs and 32 warps' histograms fit), and warps move from a task to the
 // next without a CTA barrier: a warp that finds no query group left in task
 // i goes on to task i + 1 (the other buffer), and the last warp to leave
-// task i refills its buffer with task i + 2.  The distances are computed
+// task i refills its buffer with task i + 2.  Tasks are fetched from the
+// global counter in local-index order (the refill of task i + 2 follows
+// every warp's leaving task i, hence the refill of task i + 1), so once a
+// slot finds no task none of the later ones can.  The distances are computed
 // with the same FP32 operations as dist3f, so the results equal the
 // single-buffered walk's.
 struct WalkSlot
@@ -610,8 +613,14 @@ __global__ void __launch_bounds__(1024, 1) ksg_walk_db_kernel(WalkBatch B)
     auto xyb = [&](int b) { return reinterpret_cast<float2*>(smem_raw + (size_t)b * 24 * maxT); };
     auto zb  = [&](int b) { return reinterpret_cast<float*>(smem_raw + (size_t)b * 24 * maxT + (size_t)16 * maxT); };
     unsigned char* base = smem_raw + (size_t)48 * maxT + (size_t)warp * kWalkBuckets * 32;
-    if (warp < 2)
-        walk_slot_fill(B, slot[warp], xyb(warp), zb(warp), warp, lane);
+    // A CTA's tasks must be fetched in the order of their local index: a warp
+    // stops at the first slot without a task, so no later slot may hold one.
+    // One warp therefore fills both slots, slot 0 first.
+    if (warp == 0)
+    {
+        walk_slot_fill(B, slot[0], xyb(0), zb(0), 0, lane);
+        walk_slot_fill(B, slot[1], xyb(1), zb(1), 1, lane);
+    }
     __syncthreads();
     for (int i = 0;; ++i)
     {
@@ -725,6 +734,8 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
             const int                bstar = (int)(wr & 0xFF), prefix = (int)((wr >> 8) & 0xFFFF);
             const int                m_end = (int)((wr >> 24) & 0xFFFF);
             int                      reason = (int)((wr >> 40) & 0xFF);
+            if (m_end > Llen) // not a walk result: never read past the row
+                reason = kReasonBand;
             uint32_t                 out    = kHandOver;
             const LaneSetup          u      = lane_setup(p, a1, a2, iq, i, xa, xb);
             const bool     wx = u.wx;

@@ -501,6 +501,8 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) te_finish_kernel(TeBatch
             const int                bstar = (int)(wr & 0xFF), prefix = (int)((wr >> 8) & 0xFFFF);
             const int                m_end = (int)((wr >> 24) & 0xFFFF);
             int                      reason = (int)((wr >> 40) & 0xFF);
+            if (m_end > Llen) // not a walk result: never read past the row
+                reason = kTeReasonBand;
             uint2                    out    = make_uint2(kTeHandOver, kTeHandOver);
             const TeRow   G1 = te_row(p.SG, p.PG, p, a1, iq);
             const TeRow   M1 = te_row(p.SM, p.PM, p, a1, iq);

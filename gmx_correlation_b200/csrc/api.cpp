@@ -94,16 +94,32 @@ void gc::host::pool_give(void* p, size_t bytes)
         d = attr.device;
     else
         cudaGetLastError();
+    // A full pool gives up its largest blocks for the newest one, so it holds
+    // the sizes in current use (a workload after a much larger one would
+    // otherwise allocate and free every block of every call).
+    std::vector<void*> evicted;
+    bool               kept = false;
     {
         std::lock_guard<std::mutex> lock(g_pool_mutex);
-        if (d >= 0 && d < 64 && g_pool[d].bytes + bytes <= kPoolCap)
+        if (d >= 0 && d < 64 && bytes <= kPoolCap)
         {
-            g_pool[d].blocks.emplace(bytes, p);
-            g_pool[d].bytes += bytes;
-            return;
+            DevicePool& pool = g_pool[d];
+            while (pool.bytes + bytes > kPoolCap && !pool.blocks.empty())
+            {
+                auto big = std::prev(pool.blocks.end());
+                pool.bytes -= big->first;
+                evicted.push_back(big->second);
+                pool.blocks.erase(big);
+            }
+            pool.blocks.emplace(bytes, p);
+            pool.bytes += bytes;
+            kept = true;
         }
     }
-    cudaFree(p);
+    for (void* q : evicted)
+        cudaFree(q);
+    if (!kept)
+        cudaFree(p);
 }
 
 void gc::host::pool_release()

@@ -33,7 +33,12 @@ using namespace gc::host;
 
 namespace {
 
-constexpr double kTeBatchBudget = 24.0 * (1ull << 30); // sorted rows of one wave, all trajectories
+// Sorted rows: one trajectory's query block is sized as the single-trajectory
+// plan sizes it (so every pair task holds whole rounds of the walk CTA's
+// warps); the blocks of one wave share an arena of at most kTeArenaBudget
+// bytes, or the largest block where that is larger.
+constexpr double kTeBlockBudget = 16.0 * (1ull << 30);
+constexpr double kTeArenaBudget = 32.0 * (1ull << 30);
 constexpr int    kMaxDev        = 64;
 
 gc_status capture_graph(cudaStream_t s, cudaGraphExec_t* exec, gc_status (*fn)(void*, cudaStream_t), void* ctx)
@@ -79,6 +84,7 @@ struct TeBatchPlan
     std::vector<int>                       key;
     std::vector<std::unique_ptr<TeItem>>   items;
     DevBuf<int>                            status;
+    PoolBuf<unsigned char>                 arena;
     std::vector<std::unique_ptr<TeLaunch>> groups;
     cudaStream_t                           stream = nullptr;
     cudaGraphExec_t                        exec   = nullptr;
@@ -130,10 +136,8 @@ gc_status te_create_plan(const gc_traj_view* trajs, const int* ks, int ntraj, in
     GC_TRY(bp->status.alloc((size_t)ntraj));
     for (int i = 0; i < ntraj; ++i)
         bp->items.push_back(std::make_unique<TeItem>());
-    int                 gid[4] = {-1, -1, -1, -1};
+    int                              gid[4] = {-1, -1, -1, -1};
     std::vector<std::vector<size_t>> members;
-    std::vector<double> gbytes;
-    double              total = 0.0;
     for (int i = 0; i < ntraj; ++i)
     {
         TeItem& it = *bp->items[(size_t)i];
@@ -146,18 +150,26 @@ gc_status te_create_plan(const gc_traj_view* trajs, const int* ks, int ntraj, in
         bp->key.insert(bp->key.end(), {it.natoms, it.T, it.K});
         if (!it.active)
             continue;
-        const int Nv = it.T - lag, c = te_row_class(Nv);
+        const int c = te_row_class(it.T - lag);
         if (gid[c] < 0)
         {
             gid[c] = (int)members.size();
             members.emplace_back();
-            gbytes.push_back(0.0);
         }
         members[(size_t)gid[c]].push_back((size_t)i);
-        const double b = te_row_bytes_per_query(it.natoms, Nv) * Nv;
-        gbytes[(size_t)gid[c]] += b;
-        total += b;
     }
+    // Per row class: the walk shape of its longest trajectory, each member's
+    // block size, then the (trajectory, block) pairs packed into waves by
+    // first fit in decreasing row bytes, at most one block of a trajectory
+    // per wave (its walk results and hand-over queue hold one block).
+    struct Slot
+    {
+        size_t item;
+        int    block;
+        size_t bytes;
+    };
+    std::vector<std::vector<std::vector<Slot>>> plan(members.size());
+    size_t                                      arena = 0;
     for (size_t g = 0; g < members.size(); ++g)
     {
         int maxT = 0;
@@ -166,45 +178,70 @@ gc_status te_create_plan(const gc_traj_view* trajs, const int* ks, int ntraj, in
         int  warps  = 0;
         bool staged = false;
         gc::walk_shape(maxT, &warps, &staged);
-        const int    quantum = 32 * warps;
-        const double budget  = kTeBatchBudget * gbytes[g] / total;
-        // the smallest number of waves whose sorted rows fit the group's budget
-        std::vector<int> q;
-        for (int waves = 1;; ++waves)
-        {
-            q.clear();
-            double bytes = 0.0;
-            for (size_t i : members[g])
-            {
-                const TeItem& it = *bp->items[i];
-                const int     Nv = it.T - lag;
-                int           Qb = ((Nv + waves - 1) / waves + 31) & ~31;
-                if (Qb < Nv && Qb > quantum)
-                    Qb = (Qb + quantum - 1) / quantum * quantum;
-                Qb = std::min(Qb, Nv);
-                q.push_back(Qb);
-                bytes += te_row_bytes_per_query(it.natoms, Nv) * ((Qb + 31) & ~31);
-            }
-            if (bytes <= budget || waves >= maxT)
-                break;
-        }
-        int nw = 0;
-        for (size_t m = 0; m < members[g].size(); ++m)
-        {
-            TeItem& it = *bp->items[members[g][m]];
-            it.tt      = std::make_unique<TeTraj>();
-            GC_TRY(it.tt->create(it.natoms, it.T, it.K, lag, q[m]));
-            nw = std::max(nw, it.tt->blocks());
-        }
-        std::vector<std::vector<gc::TeParams>> waves((size_t)nw);
-        std::vector<gc::TeParams>              fix;
+        std::vector<Slot> slots;
+        size_t            largest = 0;
         for (size_t i : members[g])
         {
-            TeItem& it = *bp->items[i];
+            TeItem&   it = *bp->items[i];
+            const int Nv = it.T - lag;
+            const int Q  = ksg_block_queries(2 * it.natoms, Nv, kTeBlockBudget, 32 * warps);
+            it.tt        = std::make_unique<TeTraj>();
+            GC_TRY(it.tt->create(it.natoms, it.T, it.K, lag, Q, false));
+            const size_t b = it.tt->block_row_bytes();
+            largest        = std::max(largest, b);
             for (int w = 0; w < it.tt->blocks(); ++w)
-                waves[(size_t)w].push_back(it.tt->desc(bp->status.p + i, w));
-            fix.push_back(it.tt->desc(bp->status.p + i, 0));
+                slots.push_back({i, w, b});
         }
+        std::stable_sort(slots.begin(), slots.end(), [](const Slot& a, const Slot& b) { return a.bytes > b.bytes; });
+        const size_t        cap = std::max(largest, (size_t)kTeArenaBudget);
+        std::vector<size_t> used;
+        auto&               waves = plan[g];
+        for (const Slot& sl : slots)
+        {
+            size_t w = 0;
+            for (; w < waves.size(); ++w)
+            {
+                bool clash = false;
+                for (const Slot& o : waves[w])
+                    clash = clash || o.item == sl.item;
+                if (!clash && used[w] + sl.bytes <= cap)
+                    break;
+            }
+            if (w == waves.size())
+            {
+                waves.emplace_back();
+                used.push_back(0);
+            }
+            waves[w].push_back(sl);
+            used[w] += sl.bytes;
+            arena = std::max(arena, used[w]);
+        }
+    }
+    GC_TRY(bp->arena.alloc(arena));
+    for (size_t g = 0; g < members.size(); ++g)
+    {
+        std::vector<std::vector<gc::TeParams>> waves;
+        for (const auto& wv : plan[g])
+        {
+            waves.emplace_back();
+            size_t off = 0;
+            for (const Slot& sl : wv)
+            {
+                const TeTraj&  tt   = *bp->items[sl.item]->tt;
+                const size_t   e    = (size_t)tt.natoms * tt.Qp * tt.Lpad;
+                auto           a    = [](size_t b) { return (b + 255) & ~(size_t)255; };
+                unsigned char* base = bp->arena.p + off;
+                float*         SG   = reinterpret_cast<float*>(base);
+                float*         SM   = reinterpret_cast<float*>(base + a(e * sizeof(float)));
+                uint16_t*      PG   = reinterpret_cast<uint16_t*>(base + 2 * a(e * sizeof(float)));
+                uint16_t*      PM   = reinterpret_cast<uint16_t*>(base + 2 * a(e * sizeof(float)) + a(e * sizeof(uint16_t)));
+                waves.back().push_back(tt.desc_rows(bp->status.p + sl.item, sl.block, SG, PG, SM, PM));
+                off += sl.bytes;
+            }
+        }
+        std::vector<gc::TeParams> fix;
+        for (size_t i : members[g])
+            fix.push_back(bp->items[i]->tt->desc_rows(bp->status.p + i, 0, nullptr, nullptr, nullptr, nullptr));
         auto tl = std::make_unique<TeLaunch>();
         GC_TRY(tl->build(waves, fix));
         bp->groups.push_back(std::move(tl));

@@ -71,7 +71,7 @@ double te_row_bytes_per_query(int natoms, int Nv)
     return 2.0 * natoms * (double)(((Nv - 1) + 31) & ~31) * 6.0;
 }
 
-gc_status TeTraj::create(int n, int nframes, int k, int lg, int q)
+gc_status TeTraj::create(int n, int nframes, int k, int lg, int q, bool own_rows)
 {
     natoms = n;
     T      = nframes;
@@ -93,10 +93,13 @@ gc_status TeTraj::create(int n, int nframes, int k, int lg, int q)
     Qp   = (Q + 31) & ~31;
     Lpad = ((Nv - 1) + 31) & ~31;
     const size_t rows = (size_t)n * Qp * Lpad;
-    GC_TRY(SG.alloc(rows));
-    GC_TRY(SM.alloc(rows));
-    GC_TRY(PG.alloc(rows));
-    GC_TRY(PM.alloc(rows));
+    if (own_rows)
+    {
+        GC_TRY(SG.alloc(rows));
+        GC_TRY(SM.alloc(rows));
+        GC_TRY(PG.alloc(rows));
+        GC_TRY(PM.alloc(rows));
+    }
     GC_TRY(wres.alloc((size_t)Q * npairs));
     const double hq_want = 0.01 * (double)npairs * Nv + 4096.0;
     hq_cap               = (unsigned)(hq_want < 16777216.0 ? hq_want : 16777216.0);
@@ -141,6 +144,23 @@ TeParams TeTraj::desc(int* status, int b) const
     d.walk_elems = walk_elems.p;
     d.reasons    = reasons.p;
     return d;
+}
+
+TeParams TeTraj::desc_rows(int* status, int b, float* SG_, uint16_t* PG_, float* SM_, uint16_t* PM_) const
+{
+    TeParams d = desc(status, b);
+    d.SG       = SG_;
+    d.PG       = PG_;
+    d.SM       = SM_;
+    d.PM       = PM_;
+    return d;
+}
+
+size_t TeTraj::block_row_bytes() const
+{
+    const size_t e = (size_t)natoms * Qp * Lpad;
+    auto         a = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    return 2 * a(e * sizeof(float)) + 2 * a(e * sizeof(uint16_t));
 }
 
 gc_status TeTraj::prepare(const double* d_xyz, int* status, cudaStream_t s) const

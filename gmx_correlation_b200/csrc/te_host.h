@@ -33,10 +33,16 @@ struct TeTraj
 
     // Q > 0: the walk's workspace for query blocks of Q queries; Q == 0: the
     // brute-force kernels' (coordinates, counts and digamma table only).
-    gc_status create(int natoms, int T, int K, int lag, int Q);
+    // own_rows false: the G and M rows live elsewhere (a batch's shared
+    // arena) and are passed to desc_rows.
+    gc_status create(int natoms, int T, int K, int lag, int Q, bool own_rows = true);
     int       blocks() const { return Q > 0 ? (Nv + Q - 1) / Q : 0; }
     // Descriptor of query block b; the per-trajectory (fix-up) descriptor is block 0's.
     TeParams desc(int* status, int b) const;
+    // The same with the block's rows at the given addresses.
+    TeParams desc_rows(int* status, int b, float* SG_, uint16_t* PG_, float* SM_, uint16_t* PM_) const;
+    // Bytes of one block's G and M rows (256-byte aligned parts).
+    size_t block_row_bytes() const;
     // Transpose and FP32 copy of device coordinates d_xyz, then the counters
     // cleared (stream-ordered; no allocation, graph-capturable).
     gc_status prepare(const double* d_xyz, int* status, cudaStream_t s) const;

@@ -35,7 +35,19 @@ using namespace gc::host;
 
 namespace {
 
-constexpr double kBatchBudget = 24.0 * (1ull << 30); // sorted rows of one wave, all trajectories
+// Sorted rows: one trajectory's query block is sized as the single-trajectory
+// plan sizes it, and the blocks of one wave share an arena of at most
+// kArenaBudget bytes (or the largest block, where that is larger).
+constexpr double kBlockBudget = 16.0 * (1ull << 30);
+constexpr double kArenaBudget = 32.0 * (1ull << 30);
+
+// One trajectory's query block in a wave, at an offset of the row arena.
+struct WaveSlot
+{
+    size_t item;
+    int    block;
+    size_t bytes, offset;
+};
 
 struct BatchTraj
 {
@@ -52,6 +64,7 @@ struct BatchGroup
 {
     std::vector<size_t> members; // indices into BatchPlan::t
     int                 maxT = 0, maxK = 0;
+    std::vector<std::vector<WaveSlot>> waves;
     KsgLaunch           fl;
     WalkConfig          cfg;
 };
@@ -69,6 +82,7 @@ struct BatchPlan
     int                                     device = 0, sms = 148;
     std::vector<std::unique_ptr<BatchTraj>> t;
     DevBuf<int>                             status;
+    PoolBuf<unsigned char>                  arena; // sorted rows of one wave
     std::vector<std::unique_ptr<BatchGroup>> groups;
     bool                                    tuned  = false;
     cudaStream_t                            stream = nullptr;
@@ -89,51 +103,74 @@ struct BatchPlan
 std::mutex  g_batch_mutex;
 BatchPlan*  g_batch[64] = {};
 
-// Query-block size of every trajectory for the smallest number of waves
-// whose sorted rows fit the budget.  A trajectory split into several blocks
-// gets blocks of whole rounds of the walk CTA's warps (32 x warps queries),
-// so every warp has a query group in every round of a pair's task.
-std::vector<int> batch_blocks(const std::vector<const BatchTraj*>& t, double budget)
+// Packs the (trajectory, block) pairs of a group into waves: first fit in
+// decreasing row bytes, at most one block of a trajectory per wave (its walk
+// results and hand-over queue hold one block).  Returns the largest wave's
+// bytes.
+size_t pack_waves(BatchPlan& bp, BatchGroup& g)
 {
-    int maxT = 0;
-    for (const auto* b : t)
-        maxT = std::max(maxT, b->T);
-    int warps  = 0;
-    bool staged = false;
-    gc::walk_shape(maxT, &warps, &staged);
-    const int quantum = 32 * warps;
-    for (int waves = 1;; ++waves)
+    std::vector<WaveSlot> slots;
+    size_t                largest = 0;
+    for (size_t i : g.members)
     {
-        std::vector<int> q;
-        double           bytes = 0.0;
-        for (const auto* b : t)
-        {
-            int Qb = ((b->T + waves - 1) / waves + 31) & ~31;
-            if (Qb < b->T && Qb > quantum)
-                Qb = (Qb + quantum - 1) / quantum * quantum;
-            Qb = std::min(Qb, b->T);
-            q.push_back(Qb);
-            bytes += (double)b->natoms * (((b->T - 1) + 31) & ~31) * ((Qb + 31) & ~31) * 6.0;
-        }
-        if (bytes <= budget || waves >= maxT)
-            return q;
+        const KsgTraj& ft = bp.t[i]->ft;
+        const size_t   b  = ft.block_row_bytes();
+        largest           = std::max(largest, b);
+        for (int w = 0; w < ft.blocks(); ++w)
+            slots.push_back({i, w, b, 0});
     }
+    std::stable_sort(slots.begin(), slots.end(), [](const WaveSlot& a, const WaveSlot& b) { return a.bytes > b.bytes; });
+    const size_t        cap = std::max(largest, (size_t)kArenaBudget);
+    std::vector<size_t> used;
+    size_t              most = 0;
+    g.waves.clear();
+    for (WaveSlot sl : slots)
+    {
+        size_t w = 0;
+        for (; w < g.waves.size(); ++w)
+        {
+            bool clash = false;
+            for (const WaveSlot& o : g.waves[w])
+                clash = clash || o.item == sl.item;
+            if (!clash && used[w] + sl.bytes <= cap)
+                break;
+        }
+        if (w == g.waves.size())
+        {
+            g.waves.emplace_back();
+            used.push_back(0);
+        }
+        sl.offset = used[w];
+        g.waves[w].push_back(sl);
+        used[w] += sl.bytes;
+        most = std::max(most, used[w]);
+    }
+    return most;
 }
 
 gc_status build_launch(BatchPlan& bp, BatchGroup& g, const WalkConfig& cfg)
 {
-    int nw = 0;
     for (size_t i : g.members)
-        nw = std::max(nw, bp.t[i]->ft.blocks());
-    std::vector<std::vector<gc::WalkParams>> waves((size_t)nw);
-    std::vector<gc::WalkParams>              traj;
+        GC_TRY(bp.t[i]->ft.set_pair_tile(cfg.pair_tile));
+    std::vector<std::vector<gc::WalkParams>> waves;
+    for (const auto& wv : g.waves)
+    {
+        waves.emplace_back();
+        for (const WaveSlot& sl : wv)
+        {
+            BatchTraj&     b    = *bp.t[sl.item];
+            const size_t   e    = (size_t)b.ft.natoms * b.ft.Qp * b.ft.Lpad;
+            unsigned char* base = bp.arena.p + sl.offset;
+            float*         S    = reinterpret_cast<float*>(base);
+            uint16_t*      P    = reinterpret_cast<uint16_t*>(base + ((e * sizeof(float) + 255) & ~(size_t)255));
+            waves.back().push_back(b.ft.desc_rows(b.X.p, b.cnt.p, bp.status.p + sl.item, sl.block, S, P));
+        }
+    }
+    std::vector<gc::WalkParams> traj;
     for (size_t i : g.members)
     {
         BatchTraj& b = *bp.t[i];
-        GC_TRY(b.ft.set_pair_tile(cfg.pair_tile));
-        for (int w = 0; w < b.ft.blocks(); ++w)
-            waves[(size_t)w].push_back(b.ft.desc(b.X.p, b.cnt.p, bp.status.p + i, w));
-        traj.push_back(b.ft.desc(b.X.p, b.cnt.p, bp.status.p + i, 0));
+        traj.push_back(b.ft.desc_rows(b.X.p, b.cnt.p, bp.status.p + i, 0, nullptr, nullptr));
     }
     g.cfg = cfg;
     return g.fl.build(waves, traj, cfg);
@@ -242,11 +279,9 @@ gc_status create_plan(const gc_traj_view* trajs, const int* ks, int ntraj, int d
         bp->key.insert(bp->key.end(), {b->natoms, b->T, b->K});
         bp->t.push_back(std::move(b));
     }
-    // groups by row length; each gets a share of the row budget in
-    // proportion to the sorted rows of all its queries
+    // groups by row length, each with the walk shape of its longest
+    // trajectory and single-plan query blocks packed into waves
     int gid[4] = {-1, -1, -1, -1};
-    std::vector<double> group_bytes;
-    double              total_bytes = 0.0;
     for (size_t i = 0; i < bp->t.size(); ++i)
     {
         const BatchTraj& b = *bp->t[i];
@@ -255,31 +290,30 @@ gc_status create_plan(const gc_traj_view* trajs, const int* ks, int ntraj, int d
         {
             gid[c] = (int)bp->groups.size();
             bp->groups.push_back(std::make_unique<BatchGroup>());
-            group_bytes.push_back(0.0);
         }
         BatchGroup& g = *bp->groups[(size_t)gid[c]];
         g.members.push_back(i);
         g.maxT = std::max(g.maxT, b.T);
         g.maxK = std::max(g.maxK, b.K);
-        const double all = (double)b.natoms * (((b.T - 1) + 31) & ~31) * ((b.T + 31) & ~31) * 6.0;
-        group_bytes[(size_t)gid[c]] += all;
-        total_bytes += all;
     }
-    for (size_t gi = 0; gi < bp->groups.size(); ++gi)
+    size_t arena = 0;
+    std::vector<WalkConfig> cfgs;
+    for (auto& gp : bp->groups)
     {
-        BatchGroup&                   g = *bp->groups[gi];
-        std::vector<const BatchTraj*> members;
+        BatchGroup&      g   = *gp;
+        const WalkConfig cfg = walk_config(g.maxT, g.maxK);
         for (size_t i : g.members)
-            members.push_back(bp->t[i].get());
-        const std::vector<int> q   = batch_blocks(members, kBatchBudget * group_bytes[gi] / total_bytes);
-        const WalkConfig       cfg = walk_config(g.maxT, g.maxK);
-        for (size_t m = 0; m < g.members.size(); ++m)
         {
-            BatchTraj& b = *bp->t[g.members[m]];
-            GC_TRY(b.ft.create(b.natoms, b.T, b.K, 0, b.pairs, nullptr, nullptr, q[m], cfg.pair_tile));
+            BatchTraj& b = *bp->t[i];
+            const int  Q = ksg_block_queries(b.natoms, b.T, kBlockBudget, 32 * cfg.walk_warps);
+            GC_TRY(b.ft.create(b.natoms, b.T, b.K, 0, b.pairs, nullptr, nullptr, Q, cfg.pair_tile, false, false));
         }
-        GC_TRY(build_launch(*bp, g, cfg));
+        arena = std::max(arena, pack_waves(*bp, g));
+        cfgs.push_back(cfg);
     }
+    GC_TRY(bp->arena.alloc(arena));
+    for (size_t gi = 0; gi < bp->groups.size(); ++gi)
+        GC_TRY(build_launch(*bp, *bp->groups[gi], cfgs[gi]));
     out = std::move(bp);
     return GC_OK;
 }

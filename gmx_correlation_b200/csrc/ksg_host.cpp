@@ -30,7 +30,7 @@ int ksg_block_queries(int natoms, int T, double budget, int quantum, double extr
 }
 
 gc_status KsgTraj::create(int n, int nframes, int k, long pb, long pc, const int64_t* lst, const int2* d_ab, int q,
-                          int tile, bool unsorted_rows)
+                          int tile, bool unsorted_rows, bool own_rows)
 {
     natoms     = n;
     T          = nframes;
@@ -47,8 +47,16 @@ gc_status KsgTraj::create(int n, int nframes, int k, long pb, long pc, const int
         list.assign(lst, lst + pc);
     GC_TRY(X32.alloc((size_t)natoms * T));
     GC_TRY(eps.alloc((size_t)natoms));
-    GC_TRY(S.alloc((size_t)natoms * Qp * Lpad));
-    GC_TRY(P.alloc((size_t)natoms * Qp * Lpad));
+    if (own_rows)
+    {
+        GC_TRY(S.alloc((size_t)natoms * Qp * Lpad));
+        GC_TRY(P.alloc((size_t)natoms * Qp * Lpad));
+    }
+    else
+    {
+        S.reset();
+        P.reset();
+    }
     Tpad = (T + 3) & ~3;
     if (unsorted_rows)
         GC_TRY(U.alloc((size_t)natoms * Qp * Tpad));
@@ -130,6 +138,21 @@ WalkParams KsgTraj::desc(const double* X, uint32_t* cnt, int* status, int b) con
     w.U          = U.p;
     w.Tpad       = Tpad;
     return w;
+}
+
+WalkParams KsgTraj::desc_rows(const double* X, uint32_t* cnt, int* status, int b, float* S_, uint16_t* P_) const
+{
+    WalkParams w = desc(X, cnt, status, b);
+    w.S          = S_;
+    w.P          = P_;
+    return w;
+}
+
+size_t KsgTraj::block_row_bytes() const
+{
+    const size_t e = (size_t)natoms * Qp * Lpad;
+    auto         a = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    return a(e * sizeof(float)) + a(e * sizeof(uint16_t));
 }
 
 gc_status KsgTraj::clear(cudaStream_t s)

@@ -45,13 +45,19 @@ struct KsgTraj
     int                         Tpad = 0;
 
     // Sizes the workspace for query blocks of Q frames (a multiple of 32, or T).
+    // own_rows false: the sorted rows live elsewhere (a batch's shared arena)
+    // and are passed to desc_rows.
     gc_status create(int natoms, int T, int K, long pair_begin, long pair_count, const int64_t* list,
-                     const int2* d_pair_ab, int Q, int pair_tile, bool unsorted_rows = false);
+                     const int2* d_pair_ab, int Q, int pair_tile, bool unsorted_rows = false, bool own_rows = true);
     // Reorders the pairs by atom tiles of the given side (device upload).
     gc_status set_pair_tile(int tile);
     int       blocks() const { return (T + Q - 1) / Q; }
     // Descriptor of query block b (first query b * Q).
     WalkParams desc(const double* X, uint32_t* cnt, int* status, int b) const;
+    // The same with the block's sorted rows at the given addresses.
+    WalkParams desc_rows(const double* X, uint32_t* cnt, int* status, int b, float* S_, uint16_t* P_) const;
+    // Bytes of one block's sorted rows (256-byte aligned parts: distances, then frames).
+    size_t block_row_bytes() const;
     // Clears the counters and the hand-over queue (stream-ordered).
     gc_status clear(cudaStream_t s);
 };

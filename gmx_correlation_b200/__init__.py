@@ -31,7 +31,8 @@ __all__ = [
     "write_matrix", "write_xpm_matrix", "read_matrix", "KsgPlan", "PATH_AUTO",
     "PATH_EXACT_FP64", "LIB_PATH", "probe_fp32", "screen_features", "ScreenModel", "ksg_screened",
     "SCREEN_IN", "SCREEN_RAW", "SCREEN_BASE", "SCREEN_COMP", "release_cache", "ksg_batch",
-    "ksg_batch_release",
+    "ksg_batch_release", "te_batch", "gcmi_batch", "corr_batch", "batch_release", "TePlan",
+    "read_trajectory", "write_trajectory", "trajectory_info", "read_index", "parse_atoms",
 ]
 
 LIB_PATH = Path(__file__).resolve().parent / "libgmxcorr_b200.so"
@@ -691,3 +692,6 @@ def ksg_screened(x, k: int, model: ScreenModel, *, audit_frac: float = 0.05, sig
                                  _dptr(out), ctypes.byref(rep)))
     report = {f: getattr(rep, f) for f, _ in _ScreenReport._fields_}
     return out.reshape(n, n), report
+
+
+from .trajio import parse_atoms, read_index, read_trajectory, trajectory_info, write_trajectory  # noqa: E402

@@ -4,16 +4,25 @@
 // (src/gmx_correlation.cpp:77-135 options, :247-355 writeOutput): GCMI
 // (-gcmi) before Gaussian (-linear) before KSG, pearsify unless -mi, an
 // optional transfer-entropy matrix (-te, -lag, -ote), correl.dat (-o) and
-// XPM (-m) output.  GROMACS trajectory reading is replaced by the
-// reference's own -dump text format (src/gmx_correlation.cpp:225-244):
-// a "natoms nframes" line, then per frame and atom one "x y z" line of
-// mean-centred coordinates.  It calls only the drop-in C++ interface
-// (correlation_core.h, gcmi.h, transfer_entropy.h), i.e. exactly what the
-// reference front end links against.
+// XPM (-m) output.  GROMACS trajectory reading (src/gmx_correlation.cpp:
+// 158-223) is replaced by the library's native XTC / TRR reader
+// (gc_traj_read: the atoms of an index group (-n, -sel) or of an atom-number
+// list (-sel "1-100 120"), frames inside -b / -e, every -skip-th, each atom's
+// mean subtracted as finishAnalysis does), and the reference's own -dump
+// text format (src/gmx_correlation.cpp:225-244) is read as well: a
+// "natoms nframes" line, then per frame and atom one "x y z" line of
+// mean-centred coordinates.  The estimators are called only through the
+// drop-in C++ interface (correlation_core.h, gcmi.h, transfer_entropy.h),
+// i.e. exactly what the reference front end links against.
 
 #include "correlation_core.h"
 #include "gcmi.h"
+#include "gmx_corr_b200.h"
 #include "transfer_entropy.h"
+
+#include <cmath>
+#include <fstream>
+#include <sstream>
 
 #include <chrono>
 #include <cstdio>
@@ -27,17 +36,19 @@ namespace {
 
 struct Options
 {
-    std::string in, out = "correl.dat", xpm, ote, dump, sel = "selection";
+    std::string in, out = "correl.dat", xpm, ote, dump, sel, ndx;
     int         skip = 1, k = 100, nt = 0, lag = 1;
+    double      tb = NAN, te_ = NAN;
     bool        linear = false, mi = false, gpu = false, gcmi = false, te = false, fit = false;
 };
 
 void usage()
 {
     std::fprintf(stderr,
-                 "usage: gmx_correlation_b200 -f traj_dump.txt [-o correl.dat] [-m correl.xpm] [-k 100]\n"
+                 "usage: gmx_correlation_b200 -f traj.xtc|traj.trr|traj_dump.txt [-n index.ndx] [-sel group|\"1-100\"]\n"
+                 "       [-b t0] [-e t1] [-o correl.dat] [-m correl.xpm] [-k 100]\n"
                  "       [-skip 1] [-linear] [-mi] [-gpu] [-nt 0] [-gcmi] [-te] [-lag 1] [-ote te.dat]\n"
-                 "       [-dump out_dump.txt] [-sel name]\n");
+                 "       [-dump out_dump.txt]\n");
 }
 
 bool flag(const char* a, const char* name) { return std::strcmp(a, name) == 0; }
@@ -73,6 +84,12 @@ Options parse(int argc, char** argv)
             o.dump = next();
         else if (flag(a, "-sel"))
             o.sel = next();
+        else if (flag(a, "-n"))
+            o.ndx = next();
+        else if (flag(a, "-b"))
+            o.tb = std::atof(next());
+        else if (flag(a, "-e"))
+            o.te_ = std::atof(next());
         else if (flag(a, "-linear"))
             o.linear = true;
         else if (flag(a, "-mi"))
@@ -94,7 +111,7 @@ Options parse(int argc, char** argv)
             throw std::runtime_error(std::string("unknown option ") + a);
     }
     if (o.in.empty())
-        throw std::runtime_error("-f <trajectory dump> is required");
+        throw std::runtime_error("-f <trajectory: .xtc, .trr or -dump text> is required");
     // initAnalysis checks (src/gmx_correlation.cpp:139-155)
     if (o.skip < 1)
         throw std::runtime_error("The -skip value must be at least 1.");
@@ -161,6 +178,130 @@ void read_dump(const Options& o, t_traj* traj)
     }
 }
 
+// 0-based atom indices of an index group (-n file, -sel name) or of an
+// atom-number list such as "1-100 120" (1-based, inclusive ranges).
+std::vector<int> selection(const Options& o)
+{
+    std::vector<int> atoms;
+    if (!o.ndx.empty())
+    {
+        std::ifstream f(o.ndx);
+        if (!f)
+            throw std::runtime_error("Cannot open index file " + o.ndx);
+        std::string line, group;
+        bool        found = false, in_group = false;
+        std::vector<std::string> names;
+        while (std::getline(f, line))
+        {
+            line = line.substr(0, line.find(';'));
+            const size_t l = line.find('['), r = line.find(']');
+            if (l != std::string::npos && r != std::string::npos && r > l)
+            {
+                std::string nm = line.substr(l + 1, r - l - 1);
+                nm.erase(0, nm.find_first_not_of(" \t"));
+                nm.erase(nm.find_last_not_of(" \t") + 1);
+                names.push_back(nm);
+                in_group = !found && nm == o.sel;
+                found    = found || in_group;
+                continue;
+            }
+            if (!in_group)
+                continue;
+            std::istringstream is(line);
+            long               v;
+            while (is >> v)
+            {
+                if (v < 1)
+                    throw std::runtime_error("index file " + o.ndx + ": atom number below 1");
+                atoms.push_back((int)(v - 1));
+            }
+        }
+        if (!found)
+        {
+            std::string all;
+            for (const auto& n : names)
+                all += " '" + n + "'";
+            throw std::runtime_error("-sel: no group '" + o.sel + "' in " + o.ndx + " (groups:" + all + ")");
+        }
+        if (atoms.empty())
+            throw std::runtime_error("-sel: group '" + o.sel + "' is empty");
+        return atoms;
+    }
+    if (o.sel.empty())
+        return atoms; // every atom
+    std::string spec = o.sel;
+    for (char& c : spec)
+        if (c == ',')
+            c = ' ';
+    std::istringstream is(spec);
+    std::string        tok;
+    while (is >> tok)
+    {
+        const size_t dash = tok.find('-');
+        char*        end  = nullptr;
+        const long   a    = std::strtol(tok.c_str(), &end, 10);
+        long         b    = a;
+        if (dash != std::string::npos && dash > 0)
+            b = std::strtol(tok.c_str() + dash + 1, &end, 10);
+        if (!end || *end != 0 || a < 1 || b < a)
+            throw std::runtime_error("-sel: '" + tok + "' is neither an index group (give -n) nor an atom range");
+        for (long v = a; v <= b; ++v)
+            atoms.push_back((int)(v - 1));
+    }
+    return atoms;
+}
+
+// XTC / TRR through the library reader; fills traj as finishAnalysis does.
+bool read_binary(const Options& o, t_traj* traj)
+{
+    int fmt = 0;
+    {
+        FILE* f = std::fopen(o.in.c_str(), "rb");
+        if (!f)
+            throw std::runtime_error("Cannot open trajectory: " + o.in);
+        unsigned char b[4] = {0, 0, 0, 0};
+        const size_t  n    = std::fread(b, 1, 4, f);
+        std::fclose(f);
+        const int m = n == 4 ? (b[0] << 24 | b[1] << 16 | b[2] << 8 | b[3]) : 0;
+        fmt         = m == 1995 ? GC_TRAJ_XTC : (m == 1993 ? GC_TRAJ_TRR : 0);
+    }
+    if (!fmt)
+        return false;
+    const std::vector<int> atoms = selection(o);
+    gc_traj_select         s{};
+    s.atoms  = atoms.empty() ? nullptr : atoms.data();
+    s.natoms = (int)atoms.size();
+    s.skip   = o.skip;
+    s.flags  = GC_TRAJ_CENTER;
+    if (!std::isnan(o.tb))
+    {
+        s.t_begin = o.tb;
+        s.flags |= GC_TRAJ_BEGIN;
+    }
+    if (!std::isnan(o.te_))
+    {
+        s.t_end = o.te_;
+        s.flags |= GC_TRAJ_END;
+    }
+    double* xyz = nullptr;
+    int     n = 0, T = 0;
+    if (gc_traj_read(o.in.c_str(), &s, &xyz, &n, &T) != GC_OK)
+        throw std::runtime_error(gc_last_error());
+    traj->natoms  = n;
+    traj->nframes = T;
+    snew(traj->x, n);
+    snew(traj->xav, n);
+    for (int a = 0; a < n; ++a)
+    {
+        snew(traj->x[a], T);
+        for (int t = 0; t < T; ++t)
+            for (int d = 0; d < 3; ++d)
+                traj->x[a][t][d] = xyz[((size_t)a * T + t) * 3 + d];
+    }
+    gc_traj_free(xyz);
+    return true;
+}
+
 void write_dump(const std::string& path, const t_traj& t)
 {
     FILE* dp = std::fopen(path.c_str(), "w");
@@ -176,7 +317,12 @@ void write_dump(const std::string& path, const t_traj& t)
 int run(const Options& o)
 {
     t_traj traj;
-    read_dump(o, &traj);
+    if (!read_binary(o, &traj))
+    {
+        if (!o.ndx.empty() || !o.sel.empty() || !std::isnan(o.tb) || !std::isnan(o.te_))
+            throw std::runtime_error("-n, -sel, -b and -e apply to XTC / TRR input, not to a -dump file");
+        read_dump(o, &traj);
+    }
     if (o.k >= traj.nframes)
         throw std::runtime_error("The -k value must be smaller than the number of analyzed frames.");
     if (!o.dump.empty())
@@ -238,7 +384,7 @@ int run(const Options& o)
     write_matrix(result.data(), n, o.out.c_str());
     if (!o.xpm.empty())
     {
-        const std::string title = o.sel + " correlation matrix";
+        const std::string title = (o.sel.empty() ? std::string("selection") : o.sel) + " correlation matrix";
         write_xpm_matrix(result.data(), n, o.xpm.c_str(), title.c_str(), o.mi ? "MI (bits)" : "r(MI)");
         std::fprintf(stderr, "Writing XPM to %s\n", o.xpm.c_str());
     }

@@ -400,6 +400,55 @@ gc_status gc_ksg_screened(const gc_traj_view* traj, int k, gc_screen_model* mode
  * share the one array: calls whose work overlaps on the GPU race. */
 gc_status gc_ksg_pair_mi_noalloc(const double* d_xyz, int natoms, int nframes, int k, double* d_pair_mi, void* stream);
 
+/* ---- Trajectory ingest ----------------------------------------------------
+ * Replaces the GROMACS front end's frame collection (src/gmx_correlation.cpp:
+ * 158-182 analyzeFrame: a static atom selection, every skip-th analysed
+ * frame; :184-223 finishAnalysis: per-atom mean over the kept frames, summed
+ * in frame order, subtracted).  Host-only: no device is needed.  Formats are
+ * told apart by content: GROMACS XTC (compressed, magic 1995), TRR (magic
+ * 1993, float or double; positions only, velocities and forces skipped) and
+ * the reference's -dump text file (src/gmx_correlation.cpp:225-244; frame
+ * times are the frame indices).  Positions are in the file's units (nm).
+ * XTC positions come out as GROMACS' mixed-precision reader gives them
+ * (integer times float(1/precision)); double TRR positions are rounded to
+ * float unless GC_TRAJ_KEEP_DOUBLE is set.  No periodic-boundary treatment or
+ * fitting is applied (the reference asks for a trajectory pre-fitted with
+ * gmx trjconv). */
+#define GC_TRAJ_XTC  1
+#define GC_TRAJ_TRR  2
+#define GC_TRAJ_DUMP 3
+
+#define GC_TRAJ_CENTER      1 /* subtract each atom's mean position (the reference's centring) */
+#define GC_TRAJ_KEEP_DOUBLE 2 /* read: double TRR positions unrounded; write: a double-precision TRR */
+#define GC_TRAJ_BEGIN       4 /* ignore frames with time < t_begin (GROMACS -b) */
+#define GC_TRAJ_END         8 /* ignore frames with time > t_end (GROMACS -e) */
+
+typedef struct gc_traj_select
+{
+    const int* atoms;  /* 0-based atom indices in output order (the selection); NULL: all atoms */
+    int        natoms; /* entries of atoms (0 with atoms NULL) */
+    int        skip;   /* keep every skip-th frame inside the time window, counted from the first (>= 1) */
+    double     t_begin, t_end; /* ps, with GC_TRAJ_BEGIN / GC_TRAJ_END */
+    int        flags;  /* GC_TRAJ_* flags */
+} gc_traj_select;
+
+/* Format, atom count and frame count of a trajectory (reads the whole file). */
+gc_status gc_traj_info(const char* path, int* format, int* natoms, int* nframes);
+/* Positions of the selected atoms in the kept frames as a malloc'd host array
+ * x[atom][frame][dim] (release with gc_traj_free), the layout of t_traj and
+ * of gc_traj_view.  sel NULL: all atoms, all frames, no centring.  Fails with
+ * GC_ERR_INVALID (message in gc_last_error) on a malformed or truncated
+ * frame, an atom count that changes between frames, a selected index outside
+ * the file, or no frame kept; GC_ERR_IO when the file cannot be opened. */
+gc_status gc_traj_read(const char* path, const gc_traj_select* sel, double** xyz, int* natoms, int* nframes);
+void      gc_traj_free(double* xyz);
+/* Writes nframes frames of positions xyz[frame][atom][dim] (nm) as XTC
+ * (precision: 1000 = 0.001 nm when <= 0) or TRR (float; double with
+ * GC_TRAJ_KEEP_DOUBLE in flags).  box: 9 floats per frame or NULL (zero box);
+ * times: ps per frame or NULL (the frame index); steps are frame indices. */
+gc_status gc_traj_write(const char* path, int format, const float* xyz, int natoms, int nframes, const float* box,
+                        const double* times, float precision, int flags);
+
 #ifdef __cplusplus
 }
 #endif

@@ -105,3 +105,27 @@ def test_cli_rejects_bad_options(tmp_path):
     cli = PKG / "gmx_correlation_b200"
     r = subprocess.run([str(cli), "-f", "nope.txt", "-fit"], capture_output=True, text=True)
     assert r.returncode != 0 and "fitting" in r.stderr
+
+
+def test_cli_xtc_input_matches_oracle(gc, oracle, small_x, tmp_path):
+    """XTC in, correl.dat out: the KSG matrix of the selected atoms equals the
+    oracle's on the positions the oracle's own XTC restatement decodes and
+    centres (the reference's frame collection and finishAnalysis)."""
+    from oracle import xtc as ox
+
+    cli = PKG / "gmx_correlation_b200"
+    frames = np.ascontiguousarray((small_x[:20] + 3.0).transpose(1, 0, 2)).astype(np.float32)
+    xtc = tmp_path / "traj.xtc"
+    gc.write_trajectory(xtc, frames, precision=10000.0)
+    ndx = tmp_path / "index.ndx"
+    sel = [1, 4, 5, 9, 12, 13, 17, 20]  # 1-based atom numbers
+    ndx.write_text("[ Sel ]\n" + " ".join(map(str, sel)) + "\n")
+    out = tmp_path / "correl.dat"
+    subprocess.run([str(cli), "-f", str(xtc), "-n", str(ndx), "-sel", "Sel", "-o", str(out), "-k", "10", "-mi"],
+                   check=True, capture_output=True)
+    pos = np.stack([f[3] for f in ox.read_xtc(xtc)]).transpose(1, 0, 2).astype(np.float64)
+    x = ox.center(pos[[s - 1 for s in sel]])
+    np.testing.assert_array_equal(gc.read_trajectory(xtc, [s - 1 for s in sel]), x)
+    want = tmp_path / "want.dat"
+    gc.write_matrix(oracle.ksg_matrix(x, 10), want)
+    assert out.read_bytes() == want.read_bytes()

@@ -414,6 +414,49 @@ gc_status gc_ksg_pair_mi_noalloc(const double* d_xyz, int natoms, int nframes, i
  * float unless GC_TRAJ_KEEP_DOUBLE is set.  No periodic-boundary treatment or
  * fitting is applied (the reference asks for a trajectory pre-fitted with
  * gmx trjconv). */
+/* ---- The MILCA estimator family (lib/kraskov.cpp:347-2155) ----------------
+ * One entry point per reference function, same arguments (x: one host row of
+ * N doubles per component, psi: digamma table psi[0..N], scal: per-row scale
+ * of the 1-D box counts, whose boxes (int)(x*scal) must lie in 0..N-5).  Each
+ * runs the exact FP64 neighbour search on the GPU and returns the
+ * reference's values bit for bit; like the reference, every function but
+ * redr_embed leaves the rows of x sorted by the cells of its search grid.
+ * mi_cr: 2K values, (mic, mir) for k = 1..K.  Errors: GC_ERR_INVALID (bad
+ * sizes, K >= N, a scale outside the box range), GC_ERR_NONFINITE, device
+ * errors.  Where a 1-D box count comes out at -1 (the query's own box lies
+ * outside the end boxes of [x - eps, x + eps]) the reference reads psi[-1],
+ * the word before its table; that term is taken as 0 here (= psi[0]).
+ * lib/kraskov.cpp: mi2 :347, mi2c :443, mi2r :529, red :615, redc :712,
+ * redr :799, redr_embed :883, mi_xnyn :1004, mic_xnyn :1121, mir_xnyn :1228,
+ * redK :1333, mi2K :1456, mi_xnynK :1579, mi_xnynKembed :1713, mi2h :1811,
+ * mi_d :1950, mi2r_ :2071. */
+gc_status gc_milca_mi2(double** x, int N, int K, const double* psi, const double* scal, double* mic, double* mir);
+gc_status gc_milca_mi2c(double** x, int N, int K, const double* psi, const double* scal, double* mic);
+gc_status gc_milca_mi2r(double** x, int N, int K, const double* psi, const double* scal, double* mir);
+gc_status gc_milca_mi2r_(double** x, int N, int K, const double* psi, const double* scal, double* mir);
+gc_status gc_milca_mi2K(double** x, int N, int K, const double* psi, const double* scal, double* mi_cr);
+/* also prints the reference's entropy lines to stdout */
+gc_status gc_milca_mi2h(double** x, int N, int K, const double* psi, const double* scal, double* mic, double* mir,
+                        double* hc, double* hr);
+gc_status gc_milca_red(double** x, int dim, int N, int K, const double* psi, const double* scal, double* mic,
+                       double* mir);
+gc_status gc_milca_redc(double** x, int dim, int N, int K, const double* psi, const double* scal, double* mic);
+gc_status gc_milca_redr(double** x, int dim, int N, int K, const double* psi, const double* scal, double* mir);
+gc_status gc_milca_redK(double** x, int dim, int N, int K, const double* psi, const double* scal, double* mi_cr);
+gc_status gc_milca_redr_embed(double** x, int dim, int edim, int tau, int N, int K, const double* psi, double* mir);
+gc_status gc_milca_mi_xnyn(double** x, int dimx, int dimy, int N, int K, const double* psi, const double* scal,
+                           double* mic, double* mir);
+gc_status gc_milca_mic_xnyn(double** x, int dimx, int dimy, int N, int K, const double* psi, const double* scal,
+                            double* mic);
+gc_status gc_milca_mir_xnyn(double** x, int dimx, int dimy, int N, int K, const double* psi, const double* scal,
+                            double* mir);
+gc_status gc_milca_mi_xnynK(double** x, int dimx, int dimy, int N, int K, const double* psi, const double* scal,
+                            double* mi_cr);
+/* the reference's caller-built marginal grids are not needed (exact counts) */
+gc_status gc_milca_mi_xnynKembed(double** x, int dim, int N, int K, const double* psi, double* mi_cr);
+gc_status gc_milca_mi_d(double** x, int dim, int N, int K, float* mi_cr, const double* psi, const double* phi,
+                        double minx, double maxx, double miny, double maxy);
+
 #define GC_TRAJ_XTC  1
 #define GC_TRAJ_TRR  2
 #define GC_TRAJ_DUMP 3

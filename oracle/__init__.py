@@ -154,6 +154,29 @@ class Reference:
     def max_threads(self) -> int:
         return int(self.L.gcref_max_threads())
 
+    def milca(self, name, rows, k, *, dim=None, dimx=0, dimy=0, edim=1, tau=1, psi, scal=None, phi=None,
+              minmax=(0.0, 1.0, 0.0, 1.0)):
+        """One of the reference's MILCA estimators (lib/kraskov.cpp:347-2155) on
+        rows (D, N); returns (out[4], floats[2K] for mi_d, the rows as the
+        reference leaves them).  out: mic, mir, hc, hr, or 2K values."""
+        x = np.array(rows, dtype=np.float64, order="C", copy=True)
+        D, N = x.shape
+        dim = D if dim is None else dim
+        out = np.zeros(max(4, 2 * k))
+        outf = np.zeros(2 * k, dtype=np.float32)
+        # a zero word before the table: where a 1-D box count is -1 the
+        # reference reads psi[-1]
+        psig = np.concatenate([[0.0], np.asarray(psi, dtype=np.float64)])
+        scal = np.zeros(D) if scal is None else np.ascontiguousarray(scal, dtype=np.float64)
+        phi = np.zeros(k + 1) if phi is None else np.ascontiguousarray(phi, dtype=np.float64)
+        f = self.L.gcref_milca
+        f.argtypes = [ctypes.c_char_p, ctypes.c_void_p] + [ctypes.c_int] * 8 + [ctypes.c_void_p] * 3 + \
+            [ctypes.c_double] * 4 + [ctypes.c_void_p] * 2
+        self._ok(f(name.encode(), x.ctypes.data, D, N, k, dim, dimx, dimy, edim, tau, psig.ctypes.data + 8,
+                   scal.ctypes.data, phi.ctypes.data, *[float(m) for m in minmax], out.ctypes.data,
+                   outf.ctypes.data))
+        return out, outf, x
+
     def ksg_matrix(self, x, k, nthreads=0):
         n, T = x.shape[0], x.shape[1]
         m = np.zeros(n * n)

@@ -40,6 +40,28 @@ int  neiE(double** x, int i, int comp1, int comp2, int dim, int bs, double epsgr
 void neiK(double** x, int dim, int comp1, int comp2, int i, int bs, double epsgrid, int K,
           int** box, int* lis, int* nn);
 
+// The unused MILCA estimators of lib/kraskov.cpp (:347-2155), by their own
+// definitions' signatures; gcref_milca() calls them for the parity tests.
+void mi2(double** x, int N, int K, double* psi, double* scal, double* mic, double* mir);
+void mi2c(double** x, int N, int K, double* psi, double* scal, double* mic);
+void mi2r(double** x, int N, int K, double* psi, double* scal, double* mir);
+void mi2r_(double** x, int N, int K, double* psi, double* scal, double* mir);
+void mi2K(double** x, int N, int K, double* psi, double* scal, double* mi_cr);
+void mi2h(double** x, int N, int K, double* psi, double* scal, double* mic, double* mir, double* hc, double* hr);
+void red(double** x, int dim, int N, int K, double* psi, double* scal, double* mic, double* mir);
+void redc(double** x, int dim, int N, int K, double* psi, double* scal, double* mic);
+void redr(double** x, int dim, int N, int K, double* psi, double* scal, double* mir);
+void redK(double** x, int dim, int N, int K, double* psi, double* scal, double* mi_cr);
+void redr_embed(double** x, int dim, int edim, int tau, int N, int K, double* psi, double* mir);
+void mi_xnyn(double** x, int dimx, int dimy, int N, int K, double* psi, double* scal, double* mic, double* mir);
+void mic_xnyn(double** x, int dimx, int dimy, int N, int K, double* psi, double* scal, double* mic);
+void mir_xnyn(double** x, int dimx, int dimy, int N, int K, double* psi, double* scal, double* mir);
+void mi_xnynK(double** x, int dimx, int dimy, int N, int K, double* psi, double* scal, double* mi_cr);
+void mi_xnynKembed(double** x, int dim, int N, int K, double** xx, double** yy, int** boxx, int* lisx, int* indx,
+                   int** boxy, int* lisy, int* indy, double* psi, double* mi_cr);
+void mi_d(double** x, int dim, int N, int K, float* mi_cr, double* psi, double* phi, double minx, double maxx,
+          double miny, double maxy);
+
 namespace {
 
 thread_local std::string g_err;
@@ -314,5 +336,82 @@ int gcref_ksg_matrix_legacy_gpu(const double* xyz, int natoms, int nframes, int 
     return rc;
 }
 #endif
+
+// One MILCA estimator of the reference on rows[D][N] (sorted in place by the
+// reference, as it does to its caller's rows).  dim / dimx / dimy / edim /
+// tau as the function takes them; out: mic, mir (hc, hr for mi2h) or 2K
+// values; outf: mi_d's 2K floats.  mi_xnynKembed gets the marginal copies
+// and grids the reference expects its caller to build (make_box2ind on each
+// block, BOX from N and K).
+int gcref_milca(const char* name, double* rows, int D, int N, int K, int dim, int dimx, int dimy, int edim, int tau,
+                double* psi, double* scal, double* phi, double minx, double maxx, double miny, double maxy,
+                double* out, float* outf)
+{
+    std::vector<double*> x((size_t)D);
+    for (int d = 0; d < D; ++d)
+        x[(size_t)d] = rows + (size_t)d * N;
+    const std::string n(name);
+    return guarded([&] {
+        double** X = x.data();
+        if (n == "mi2")
+            mi2(X, N, K, psi, scal, out, out + 1);
+        else if (n == "mi2c")
+            mi2c(X, N, K, psi, scal, out);
+        else if (n == "mi2r")
+            mi2r(X, N, K, psi, scal, out + 1);
+        else if (n == "mi2r_")
+            mi2r_(X, N, K, psi, scal, out + 1);
+        else if (n == "mi2K")
+            mi2K(X, N, K, psi, scal, out);
+        else if (n == "mi2h")
+            mi2h(X, N, K, psi, scal, out, out + 1, out + 2, out + 3);
+        else if (n == "red")
+            red(X, dim, N, K, psi, scal, out, out + 1);
+        else if (n == "redc")
+            redc(X, dim, N, K, psi, scal, out);
+        else if (n == "redr")
+            redr(X, dim, N, K, psi, scal, out + 1);
+        else if (n == "redK")
+            redK(X, dim, N, K, psi, scal, out);
+        else if (n == "redr_embed")
+            redr_embed(X, dim, edim, tau, N, K, psi, out + 1);
+        else if (n == "mi_xnyn")
+            mi_xnyn(X, dimx, dimy, N, K, psi, scal, out, out + 1);
+        else if (n == "mic_xnyn")
+            mic_xnyn(X, dimx, dimy, N, K, psi, scal, out);
+        else if (n == "mir_xnyn")
+            mir_xnyn(X, dimx, dimy, N, K, psi, scal, out + 1);
+        else if (n == "mi_xnynK")
+            mi_xnynK(X, dimx, dimy, N, K, psi, scal, out);
+        else if (n == "mi_d")
+            mi_d(X, dim, N, K, outf, psi, phi, minx, maxx, miny, maxy);
+        else if (n == "mi_xnynKembed")
+        {
+            int BOX = 1;
+            while (0.5 * BOX * BOX * K < N)
+                BOX *= 2;
+            std::vector<std::vector<double>> cx((size_t)dim), cy((size_t)dim);
+            std::vector<double*>             xx((size_t)dim), yy((size_t)dim);
+            for (int d = 0; d < dim; ++d)
+            {
+                cx[(size_t)d].assign(X[d], X[d] + N);
+                cy[(size_t)d].assign(X[dim + d], X[dim + d] + N);
+                xx[(size_t)d] = cx[(size_t)d].data();
+                yy[(size_t)d] = cy[(size_t)d].data();
+            }
+            int**            bx = alloc_box(BOX);
+            int**            by = alloc_box(BOX);
+            std::vector<int> lx((size_t)N), ly((size_t)N), ixv((size_t)N), iyv((size_t)N);
+            make_box2ind(xx.data(), dim, N, 0, dim - 1, BOX, BOX / 4, ixv.data(), bx, lx.data());
+            make_box2ind(yy.data(), dim, N, 0, dim - 1, BOX, BOX / 4, iyv.data(), by, ly.data());
+            mi_xnynKembed(X, dim, N, K, xx.data(), yy.data(), bx, lx.data(), ixv.data(), by, ly.data(), iyv.data(), psi,
+                          out);
+            free_box(bx, BOX);
+            free_box(by, BOX);
+        }
+        else
+            throw std::runtime_error("unknown MILCA function " + n);
+    });
+}
 
 } // extern "C"

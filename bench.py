@@ -383,13 +383,17 @@ def te_variant(gc, torch, x, k: int, lag: int, dev, local: int, mix_ops: float, 
     d_te = torch.zeros((n, n), dtype=torch.float64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     plan = gc.TePlan(n, T, k, lag, device=local)
-    stream = torch.cuda.current_stream(dev)
+    # a real stream handle: the legacy default stream is handle 0, which the
+    # plan reads as "the library's own stream", and the events would then
+    # bracket nothing
+    stream = torch.cuda.Stream(dev)
     plan.run(d_xyz.data_ptr(), d_te.data_ptr(), stream.cuda_stream)
     torch.cuda.synchronize(dev)
     plan.sync()
     step, kern = [], []
     for _ in range(reps):
-        flush.zero_()
+        with torch.cuda.stream(stream):
+            flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)

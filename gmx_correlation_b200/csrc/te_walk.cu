@@ -691,6 +691,77 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) te_finish_kernel(TeBatch
     }
 }
 
+// n_ypxp of query iq of a staged pair task (x1, x2: the pair's FP32 rows,
+// in shared or global memory): the body of both count kernels.
+__device__ __forceinline__ void te_count_query(const TeParams& p, const TeTask& tk, int iq, const float4* x1,
+                                               const float4* x2, float e1, float e2a)
+{
+    const int T = p.T, Nv = p.Nv;
+    const int    qi = p.i0 + iq;
+    uint2* const cp = p.cnt + (size_t)tk.pl * Nv + qi;
+    const uint2  c  = *cp;
+    if (c.x != kTeHandOver)
+    {
+        const double eps = __longlong_as_double((long long)p.wres[(size_t)tk.pl * p.Q + iq]);
+        const int    ne  = (int)(c.y & 0xFFFFu);
+        const bool   on1 = (c.y & kTeCountOn1) != 0u;
+        const double es = on1 ? (double)e1 : (double)e2a, eo = on1 ? (double)e2a : (double)e1;
+        const float  tlo_s = __double2float_rd(__dsub_rd(eps, es));
+        const float  tlo_o = __double2float_rd(__dsub_rd(eps, eo));
+        const float  thi_o = __double2float_ru(__dadd_ru(eps, eo));
+        const TeRow  er = te_row(p.SM, p.PM, p, on1 ? tk.a1 : tk.a2, iq);
+        const float4* ox = on1 ? x2 : x1;
+        const float4  oq = ox[qi];
+        const float4* Sg = reinterpret_cast<const float4*>(er.S);
+        const uint2*  Pg = reinterpret_cast<const uint2*>(er.P);
+        const size_t  gs = (size_t)p.Qp;
+        const int     ng = (ne + 3) >> 2;
+        int           n  = 0;
+        float4        s4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint2         j4 = make_uint2(0u, 0u);
+        if (ng > 0)
+        {
+            s4 = Sg[0];
+            j4 = Pg[0];
+        }
+        for (int g0 = 0; g0 < ng; ++g0)
+        {
+            // the next group is loaded while this one is counted
+            const int    nx  = g0 + 1 < ng ? g0 + 1 : g0;
+            const float4 ns4 = Sg[(size_t)nx * gs];
+            const uint2  nj4 = Pg[(size_t)nx * gs];
+            const float  sv[4] = {s4.x, s4.y, s4.z, s4.w};
+            const unsigned jv[4] = {j4.x & 0xFFFFu, j4.x >> 16, j4.y & 0xFFFFu, j4.y >> 16};
+            unsigned     amb = 0u;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+                const bool  in = g0 * 4 + q < ne;
+                const float ov = te3(oq, ox[jv[q]]);
+                if (in && sv[q] < tlo_s && ov < tlo_o)
+                    ++n;
+                else if (in && ov <= thi_o)
+                    amb |= 1u << q;
+            }
+            for (; amb; amb &= amb - 1) // rare: FP64 on the raw coordinates
+            {
+                const int     j  = (int)u2at16(j4, __ffs(amb) - 1);
+                const double* ra = p.XT + (size_t)tk.a1 * 3 * T;
+                const double* rb = p.XT + (size_t)tk.a2 * 3 * T;
+                double        d  = 0.0;
+#pragma unroll 1
+                for (int c3 = 0; c3 < 3; ++c3)
+                    d = fmax(d, fmax(fabs(ra[c3 * T + qi] - ra[c3 * T + j]),
+                                     fabs(rb[c3 * T + qi] - rb[c3 * T + j])));
+                n += d < eps;
+            }
+            s4 = ns4;
+            j4 = nj4;
+        }
+        cp->y = (unsigned)n;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // n_ypxp = #{j : max(D1(qi, j), Y(qi, j)) < eps}: one ordered pair per CTA
 // task with its two coordinate rows staged in shared memory (the walk's
@@ -741,73 +812,132 @@ __global__ void __launch_bounds__(1024, 1) te_count_kernel(TeBatch B)
                 break;
             const int iq = g * 32 + lane;
             if (iq < p.Q)
-            {
-                const int    qi = p.i0 + iq;
-                uint2* const cp = p.cnt + (size_t)tk.pl * Nv + qi;
-                const uint2  c  = *cp;
-                if (c.x != kTeHandOver)
-                {
-                    const double eps = __longlong_as_double((long long)p.wres[(size_t)tk.pl * p.Q + iq]);
-                    const int    ne  = (int)(c.y & 0xFFFFu);
-                    const bool   on1 = (c.y & kTeCountOn1) != 0u;
-                    const double es = on1 ? (double)e1 : (double)e2a, eo = on1 ? (double)e2a : (double)e1;
-                    const float  tlo_s = __double2float_rd(__dsub_rd(eps, es));
-                    const float  tlo_o = __double2float_rd(__dsub_rd(eps, eo));
-                    const float  thi_o = __double2float_ru(__dadd_ru(eps, eo));
-                    const TeRow  er = te_row(p.SM, p.PM, p, on1 ? tk.a1 : tk.a2, iq);
-                    const float4* ox = on1 ? x2 : x1;
-                    const float4  oq = ox[qi];
-                    const float4* Sg = reinterpret_cast<const float4*>(er.S);
-                    const uint2*  Pg = reinterpret_cast<const uint2*>(er.P);
-                    const size_t  gs = (size_t)p.Qp;
-                    const int     ng = (ne + 3) >> 2;
-                    int           n  = 0;
-                    float4        s4 = make_float4(0.f, 0.f, 0.f, 0.f);
-                    uint2         j4 = make_uint2(0u, 0u);
-                    if (ng > 0)
-                    {
-                        s4 = Sg[0];
-                        j4 = Pg[0];
-                    }
-                    for (int g0 = 0; g0 < ng; ++g0)
-                    {
-                        // the next group is loaded while this one is counted
-                        const int    nx  = g0 + 1 < ng ? g0 + 1 : g0;
-                        const float4 ns4 = Sg[(size_t)nx * gs];
-                        const uint2  nj4 = Pg[(size_t)nx * gs];
-                        const float  sv[4] = {s4.x, s4.y, s4.z, s4.w};
-                        const unsigned jv[4] = {j4.x & 0xFFFFu, j4.x >> 16, j4.y & 0xFFFFu, j4.y >> 16};
-                        unsigned     amb = 0u;
-#pragma unroll
-                        for (int q = 0; q < 4; ++q)
-                        {
-                            const bool  in = g0 * 4 + q < ne;
-                            const float ov = te3(oq, ox[jv[q]]);
-                            if (in && sv[q] < tlo_s && ov < tlo_o)
-                                ++n;
-                            else if (in && ov <= thi_o)
-                                amb |= 1u << q;
-                        }
-                        for (; amb; amb &= amb - 1) // rare: FP64 on the raw coordinates
-                        {
-                            const int     j  = (int)u2at16(j4, __ffs(amb) - 1);
-                            const double* ra = p.XT + (size_t)tk.a1 * 3 * T;
-                            const double* rb = p.XT + (size_t)tk.a2 * 3 * T;
-                            double        d  = 0.0;
-#pragma unroll 1
-                            for (int c3 = 0; c3 < 3; ++c3)
-                                d = fmax(d, fmax(fabs(ra[c3 * T + qi] - ra[c3 * T + j]),
-                                                 fabs(rb[c3 * T + qi] - rb[c3 * T + j])));
-                            n += d < eps;
-                        }
-                        s4 = ns4;
-                        j4 = nj4;
-                    }
-                    cp->y = (unsigned)n;
-                }
-            }
+                te_count_query(p, tk, iq, x1, x2, e1, e2a);
         }
         __syncthreads(); // every warp is done with the staged rows
+    }
+}
+
+// A staged pair task of the double-buffered count kernel.
+struct TeSlot
+{
+    long long    t;    // global task, or -1: no more tasks
+    int          desc; // descriptor of the task
+    int          next; // query groups handed out
+    int          left; // warps done with the task
+    volatile int gen;  // CTA-local index of the task this slot holds
+    TeTask       tk;
+};
+
+// Fills slot S with the next global task as CTA-local task `gen`: one warp
+// (lane 0 takes the task, all lanes copy the pair's two FP32 rows).
+__device__ __forceinline__ void te_slot_fill(const TeBatch& B, long long total, TeSlot& S, float4* rows, int gen,
+                                             int lane)
+{
+    long long t = 0;
+    int       d = 0;
+    if (lane == 0)
+    {
+        t = (long long)atomicAdd(B.counter, 1ull);
+        if (t < total)
+            d = te_desc_of(B.wprefix, B.n, t);
+        else
+            t = -1;
+    }
+    t = __shfl_sync(kFull, t, 0);
+    d = __shfl_sync(kFull, d, 0);
+    TeTask tk{};
+    if (t >= 0)
+    {
+        const TeParams& p  = B.d[d];
+        const long long lt = t - B.wprefix[d];
+        tk.c               = (int)(lt / p.pair_count);
+        te_pair(p, (long)(lt - (long long)tk.c * p.pair_count), tk.pl, tk.a1, tk.a2);
+        const int     T  = p.T;
+        const float4* x1 = p.X32 + (size_t)tk.a1 * T;
+        const float4* x2 = p.X32 + (size_t)tk.a2 * T;
+        for (int e = lane; e < T; e += 32)
+        {
+            rows[e]     = x1[e];
+            rows[T + e] = x2[e];
+        }
+    }
+    __syncwarp();
+    if (lane == 0)
+    {
+        S.t    = t;
+        S.desc = d;
+        S.tk   = tk;
+        S.next = 0;
+        S.left = 0;
+        __threadfence_block(); // the rows and fields before the generation
+        S.gen = gen;
+    }
+    __syncwarp();
+}
+
+// The count kernel with two staged pair tasks per CTA (2 x 2 x maxT float4):
+// a warp done with its query groups of task i moves on to task i + 1 without
+// waiting for the CTA; the last warp to leave task i refills its buffer with
+// task i + 2.  Tasks reach a CTA in its local index order (one warp fills
+// both buffers first), so a warp stops at the first slot without a task.
+__global__ void __launch_bounds__(1024, 1) te_count_db_kernel(TeBatch B)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ TeSlot slot[2];
+    const int         warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const long long   total = B.wprefix[B.n];
+    auto              rows  = [&](int b) { return reinterpret_cast<float4*>(smem_raw) + (size_t)b * 2 * B.maxT; };
+    if (warp == 0)
+    {
+        te_slot_fill(B, total, slot[0], rows(0), 0, lane);
+        te_slot_fill(B, total, slot[1], rows(1), 1, lane);
+    }
+    __syncthreads();
+    for (int i = 0;; ++i)
+    {
+        const int b = i & 1;
+        TeSlot&   S = slot[b];
+        // bounded wait for the refilling warp (resident, never waiting itself)
+        int spins = 0;
+        while (S.gen != i)
+        {
+            if (++spins > (1 << 24))
+            {
+                if (lane == 0)
+                    atomicOr(B.d[0].status, kStatTimeout);
+                return;
+            }
+            __nanosleep(64);
+        }
+        __threadfence_block();
+        if (S.t < 0)
+            break;
+        const TeParams& p       = B.d[S.desc];
+        const TeTask    tk      = S.tk;
+        const int       ngroups = (p.Q + 31) >> 5;
+        const float4*   x1      = rows(b);
+        const float4*   x2      = x1 + p.T;
+        const float     e1 = p.eps_atom[tk.a1], e2a = p.eps_atom[tk.a2];
+        for (;;)
+        {
+            int gi = 0;
+            if (lane == 0)
+                gi = atomicAdd(&S.next, 1);
+            gi          = __shfl_sync(kFull, gi, 0);
+            const int g = tk.c * B.chunk + gi;
+            if (gi >= B.chunk || g >= ngroups)
+                break;
+            const int iq = g * 32 + lane;
+            if (iq < p.Q)
+                te_count_query(p, tk, iq, x1, x2, e1, e2a);
+        }
+        int last = 0;
+        if (lane == 0)
+            last = atomicAdd(&S.left, 1) == nwarps - 1;
+        last = __shfl_sync(kFull, last, 0);
+        if (last) // every warp has left task i: its buffer takes task i + 2
+            te_slot_fill(B, total, S, rows(b), i + 2, lane);
     }
 }
 
@@ -970,8 +1100,12 @@ cudaError_t launch_te_finish(const TeBatch& b, int sms, cudaStream_t s)
 
 cudaError_t launch_te_count(const TeBatch& b, int warps, bool staged, int sms, cudaStream_t s)
 {
-    void (*kernel)(TeBatch) = staged ? te_count_kernel<true> : te_count_kernel<false>;
-    const size_t smem = staged ? (size_t)2 * b.maxT * 16 : 0;
+    // two staged pair tasks per CTA where they fit (rows of up to 3584
+    // frames), else one
+    const size_t db      = (size_t)4 * b.maxT * 16;
+    const bool   dbuf    = staged && db <= (size_t)224 * 1024;
+    void (*kernel)(TeBatch) = dbuf ? te_count_db_kernel : (staged ? te_count_kernel<true> : te_count_kernel<false>);
+    const size_t smem = dbuf ? db : (staged ? (size_t)2 * b.maxT * 16 : 0);
     cudaError_t  e    = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;

@@ -230,6 +230,181 @@ __device__ __forceinline__ bool te_next_task(const TeBatch& B, long long total, 
 // staged frames) and histogram the joint value max(s, other).  STAGED: the
 // pair's two coordinate rows in shared memory.  LO (every k < 256): values
 // below L counted in histogram index 0.
+// An atom's FP32 coordinate row as float4 (global or shared memory) ...
+struct TeRows4
+{
+    const float4* x;
+    __device__ __forceinline__ float4 at(int j) const { return x[j]; }
+    __device__ __forceinline__ float  d3(const float4& q, int j) const { return te3(q, x[j]); }
+};
+
+// ... or as x,y float2 and z float in shared memory (12 bytes a frame).
+struct TeRows12
+{
+    const float2* xy;
+    const float*  z;
+    __device__ __forceinline__ float4 at(int j) const
+    {
+        const float2 v = xy[j];
+        return make_float4(v.x, v.y, z[j], 0.0f);
+    }
+    __device__ __forceinline__ float d3(const float4& q, int j) const
+    {
+        const float2 v = xy[j];
+        return fmaxf(fmaxf(fabsf(q.x - v.x), fabsf(q.y - v.y)), fabsf(q.z - z[j]));
+    }
+};
+
+// Walk of query group g of a staged pair task (x1, x2: the pair's FP32
+// rows; base: this warp's histogram): the body of both walk kernels.
+template <bool LO, class V>
+__device__ __forceinline__ void te_walk_group(const TeParams& p, const TeTask& tk, int g, const V& x1, const V& x2,
+                                              unsigned char* base, int lane)
+{
+    uint8_t*           hist = base + lane * 4;
+    auto               H    = [hist](unsigned b) -> uint8_t& { return hist[(b >> 2) * 128 + (b & 3)]; };
+    constexpr unsigned kTop = kWalkBuckets - 1;
+    const float        inf  = __int_as_float(0x7f800000);
+    const int          K = p.K, lag = p.lag, Llen = p.Nv - 1, shift = p.shift;
+    const float        ebig = fmaxf(p.eps_atom[tk.a1], p.eps_atom[tk.a2]);
+    const float        e2   = __fmul_ru(2.0f, ebig);
+    const int   iq   = g * 32 + lane;
+    const bool  live = iq < p.Q;
+    const int   iql  = live ? iq : 0;
+    const int   qi   = p.i0 + iql;
+    const TeRow G1   = te_row(p.SG, p.PG, p, tk.a1, iql);
+    const TeRow M2   = te_row(p.SM, p.PM, p, tk.a2, iql);
+    const float gk = G1.s(K - 1), yk = M2.s(K - 1);
+    const bool  wg = gk >= yk; // walk the target's G row (gather the source's Y)
+    const TeRow rw = wg ? G1 : M2;
+    const float L  = wg ? gk : yk;
+    const unsigned Lb = __float_as_uint(L);
+    // other distance of frame j: Y = |y(qi) - y(j)| or G = max over the
+    // target's past (qi, j) and future (qi + lag, j + lag)
+    const V&      oa = wg ? x2 : x1;
+    const float4  oq = oa.at(qi);
+    const float4  fq = x1.at(qi + lag);
+    {
+        uint4* h4 = reinterpret_cast<uint4*>(base);
+        for (int e = lane; e < kWalkBuckets * 32 / 16; e += 32)
+            h4[e] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    __syncwarp();
+    const unsigned Lh   = LO ? Lb - (1u << shift) : Lb;
+    auto           hidx = [Lh, shift](float v) -> unsigned {
+        if (LO)
+            return (unsigned)min(max((int)(__float_as_uint(v) - Lh) >> shift, 0), (int)kTop);
+        return min((__float_as_uint(v) - Lh) >> shift, kTop);
+    };
+    const float4* Sg = reinterpret_cast<const float4*>(rw.S);
+    const uint2*  Pg = reinterpret_cast<const uint2*>(rw.P);
+    const size_t  gs = (size_t)p.Qp;
+    int           m_end = 0, cnt_lo = 0, Rs = 0, thr = 0, grp = 0;
+    unsigned      wrap = 0u;
+    float         stop = inf;
+    bool          walking = live;
+    float4        s4      = make_float4(inf, inf, inf, inf);
+    uint2         j4      = make_uint2(0u, 0u);
+    if (live)
+    {
+        s4 = Sg[0];
+        j4 = Pg[0];
+    }
+    const int last = (Llen - 1) >> 2;
+    while (walking)
+    {
+        if (grp > last)
+        {
+            m_end = Llen;
+            break;
+        }
+        const int      nxt   = grp < last ? grp + 1 : grp;
+        const float4   ns4   = Sg[(size_t)nxt * gs];
+        const uint2    nj4   = Pg[(size_t)nxt * gs];
+        const float    sv[4] = {s4.x, s4.y, s4.z, s4.w};
+        const unsigned jv[4] = {j4.x & 0xFFFFu, j4.x >> 16, j4.y & 0xFFFFu, j4.y >> 16};
+        bool           tkn[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+        {
+            tkn[q] = sv[q] <= stop;
+            float o = oa.d3(oq, (int)jv[q]);
+            if (!wg)
+                o = fmaxf(o, x1.d3(fq, (int)jv[q] + lag));
+            const float v   = fmaxf(sv[q], o);
+            bool        inc = tkn[q];
+            if (!LO)
+            {
+                const bool below = v < L;
+                cnt_lo += inc && below;
+                inc = inc && !below;
+            }
+            uint8_t&       c  = H(hidx(v));
+            const unsigned h1 = (unsigned)c + (inc ? 1u : 0u);
+            c                 = (uint8_t)h1;
+            wrap |= h1;
+        }
+        ++grp;
+        if (!tkn[3])
+        {
+            walking = false;
+            m_end   = (grp - 1) * 4 + (int)tkn[0] + (int)tkn[1] + (int)tkn[2];
+        }
+        else if ((grp & 3) == 0)
+        {
+            H(kTop) = 0;
+            if (stop == inf)
+            {
+                const float sl = sv[3];
+                const int   bn = (LO || sl >= L) ? (int)hidx(sl) : 0;
+                for (int b = thr; b < bn; ++b)
+                    Rs += H(b);
+                thr = max(thr, bn);
+                if (cnt_lo + Rs >= K)
+                    stop = __fadd_ru(__uint_as_float(Lh + ((unsigned)bn << shift)), e2);
+            }
+        }
+        s4 = ns4;
+        j4 = nj4;
+    }
+    if (live)
+    {
+        int bstar, prefix;
+        if (stop != inf)
+        {
+            int cum = cnt_lo + Rs, b = thr - 1;
+            while (b > 0 && cum - (int)H(b) >= K)
+            {
+                cum -= H(b);
+                --b;
+            }
+            bstar  = b;
+            prefix = cum - H(b);
+        }
+        else
+        {
+            int cum = cnt_lo, b = 0;
+            while (b < (int)kTop && cum + (int)H(b) < K)
+            {
+                cum += H(b);
+                ++b;
+            }
+            bstar  = b;
+            prefix = cum;
+        }
+        const int reason = (wrap > 255u || (LO && bstar == 0)) ? kTeReasonBand
+                           : (bstar >= (int)kTop ? kTeReasonRange : 0);
+        p.wres[(size_t)tk.pl * p.Q + iq] = te_pack_walk(LO ? bstar - 1 : bstar, prefix, m_end, reason);
+    }
+    if (p.walk_elems)
+    {
+        const unsigned we = __reduce_add_sync(kFull, live ? (unsigned)m_end : 0u);
+        if (lane == 0 && we)
+            atomicAdd(p.walk_elems, (unsigned long long)we);
+    }
+    __syncwarp();
+}
+
 template <bool STAGED, bool LO>
 __global__ void __launch_bounds__(1024, 1) te_walk_kernel(TeBatch B)
 {
@@ -239,18 +414,14 @@ __global__ void __launch_bounds__(1024, 1) te_walk_kernel(TeBatch B)
     const int            warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float4*              sx   = reinterpret_cast<float4*>(smem_raw);
     unsigned char*       base = smem_raw + (STAGED ? (size_t)2 * B.maxT * 16 : 0) + (size_t)warp * kWalkBuckets * 32;
-    uint8_t*             hist = base + lane * 4;
-    auto                 H    = [hist](unsigned b) -> uint8_t& { return hist[(b >> 2) * 128 + (b & 3)]; };
-    constexpr unsigned   kTop = kWalkBuckets - 1;
 
     const long long total = B.wprefix[B.n];
-    const float     inf   = __int_as_float(0x7f800000);
     TeTask          tk;
     int             dsc;
     while (te_next_task(B, total, &s_task, &s_desc, &s_next, tk, dsc))
     {
         const TeParams& p       = B.d[dsc];
-        const int       T = p.T, K = p.K, lag = p.lag, Llen = p.Nv - 1, shift = p.shift;
+        const int       T       = p.T;
         const int       ngroups = (p.Q + 31) >> 5;
         const float4*   x1      = p.X32 + (size_t)tk.a1 * T;
         const float4*   x2      = p.X32 + (size_t)tk.a2 * T;
@@ -265,8 +436,6 @@ __global__ void __launch_bounds__(1024, 1) te_walk_kernel(TeBatch B)
             x1 = sx;
             x2 = sx + T;
         }
-        const float ebig = fmaxf(p.eps_atom[tk.a1], p.eps_atom[tk.a2]);
-        const float e2   = __fmul_ru(2.0f, ebig);
         for (;;)
         {
             int gi = 0;
@@ -276,141 +445,7 @@ __global__ void __launch_bounds__(1024, 1) te_walk_kernel(TeBatch B)
             const int g = tk.c * B.chunk + gi;
             if (gi >= B.chunk || g >= ngroups)
                 break;
-            const int   iq   = g * 32 + lane;
-            const bool  live = iq < p.Q;
-            const int   iql  = live ? iq : 0;
-            const int   qi   = p.i0 + iql;
-            const TeRow G1   = te_row(p.SG, p.PG, p, tk.a1, iql);
-            const TeRow M2   = te_row(p.SM, p.PM, p, tk.a2, iql);
-            const float gk = G1.s(K - 1), yk = M2.s(K - 1);
-            const bool  wg = gk >= yk; // walk the target's G row (gather the source's Y)
-            const TeRow rw = wg ? G1 : M2;
-            const float L  = wg ? gk : yk;
-            const unsigned Lb = __float_as_uint(L);
-            // other distance of frame j: Y = |y(qi) - y(j)| or G = max over the
-            // target's past (qi, j) and future (qi + lag, j + lag)
-            const float4* oa = wg ? x2 : x1;
-            const float4  oq = wg ? x2[qi] : x1[qi];
-            const float4  fq = x1[qi + lag];
-            {
-                uint4* h4 = reinterpret_cast<uint4*>(base);
-                for (int e = lane; e < kWalkBuckets * 32 / 16; e += 32)
-                    h4[e] = make_uint4(0u, 0u, 0u, 0u);
-            }
-            __syncwarp();
-            const unsigned Lh   = LO ? Lb - (1u << shift) : Lb;
-            auto           hidx = [Lh, shift](float v) -> unsigned {
-                if (LO)
-                    return (unsigned)min(max((int)(__float_as_uint(v) - Lh) >> shift, 0), (int)kTop);
-                return min((__float_as_uint(v) - Lh) >> shift, kTop);
-            };
-            const float4* Sg = reinterpret_cast<const float4*>(rw.S);
-            const uint2*  Pg = reinterpret_cast<const uint2*>(rw.P);
-            const size_t  gs = (size_t)p.Qp;
-            int           m_end = 0, cnt_lo = 0, Rs = 0, thr = 0, grp = 0;
-            unsigned      wrap = 0u;
-            float         stop = inf;
-            bool          walking = live;
-            float4        s4      = make_float4(inf, inf, inf, inf);
-            uint2         j4      = make_uint2(0u, 0u);
-            if (live)
-            {
-                s4 = Sg[0];
-                j4 = Pg[0];
-            }
-            const int last = (Llen - 1) >> 2;
-            while (walking)
-            {
-                if (grp > last)
-                {
-                    m_end = Llen;
-                    break;
-                }
-                const int      nxt   = grp < last ? grp + 1 : grp;
-                const float4   ns4   = Sg[(size_t)nxt * gs];
-                const uint2    nj4   = Pg[(size_t)nxt * gs];
-                const float    sv[4] = {s4.x, s4.y, s4.z, s4.w};
-                const unsigned jv[4] = {j4.x & 0xFFFFu, j4.x >> 16, j4.y & 0xFFFFu, j4.y >> 16};
-                bool           tkn[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                {
-                    tkn[q] = sv[q] <= stop;
-                    float o = te3(oq, oa[jv[q]]);
-                    if (!wg)
-                        o = fmaxf(o, te3(fq, x1[jv[q] + lag]));
-                    const float v   = fmaxf(sv[q], o);
-                    bool        inc = tkn[q];
-                    if (!LO)
-                    {
-                        const bool below = v < L;
-                        cnt_lo += inc && below;
-                        inc = inc && !below;
-                    }
-                    uint8_t&       c  = H(hidx(v));
-                    const unsigned h1 = (unsigned)c + (inc ? 1u : 0u);
-                    c                 = (uint8_t)h1;
-                    wrap |= h1;
-                }
-                ++grp;
-                if (!tkn[3])
-                {
-                    walking = false;
-                    m_end   = (grp - 1) * 4 + (int)tkn[0] + (int)tkn[1] + (int)tkn[2];
-                }
-                else if ((grp & 3) == 0)
-                {
-                    H(kTop) = 0;
-                    if (stop == inf)
-                    {
-                        const float sl = sv[3];
-                        const int   bn = (LO || sl >= L) ? (int)hidx(sl) : 0;
-                        for (int b = thr; b < bn; ++b)
-                            Rs += H(b);
-                        thr = max(thr, bn);
-                        if (cnt_lo + Rs >= K)
-                            stop = __fadd_ru(__uint_as_float(Lh + ((unsigned)bn << shift)), e2);
-                    }
-                }
-                s4 = ns4;
-                j4 = nj4;
-            }
-            if (live)
-            {
-                int bstar, prefix;
-                if (stop != inf)
-                {
-                    int cum = cnt_lo + Rs, b = thr - 1;
-                    while (b > 0 && cum - (int)H(b) >= K)
-                    {
-                        cum -= H(b);
-                        --b;
-                    }
-                    bstar  = b;
-                    prefix = cum - H(b);
-                }
-                else
-                {
-                    int cum = cnt_lo, b = 0;
-                    while (b < (int)kTop && cum + (int)H(b) < K)
-                    {
-                        cum += H(b);
-                        ++b;
-                    }
-                    bstar  = b;
-                    prefix = cum;
-                }
-                const int reason = (wrap > 255u || (LO && bstar == 0)) ? kTeReasonBand
-                                   : (bstar >= (int)kTop ? kTeReasonRange : 0);
-                p.wres[(size_t)tk.pl * p.Q + iq] = te_pack_walk(LO ? bstar - 1 : bstar, prefix, m_end, reason);
-            }
-            if (p.walk_elems)
-            {
-                const unsigned we = __reduce_add_sync(kFull, live ? (unsigned)m_end : 0u);
-                if (lane == 0 && we)
-                    atomicAdd(p.walk_elems, (unsigned long long)we);
-            }
-            __syncwarp();
+            te_walk_group<LO>(p, tk, g, TeRows4{x1}, TeRows4{x2}, base, lane);
         }
         __syncthreads();
     }
@@ -830,9 +865,11 @@ struct TeSlot
 };
 
 // Fills slot S with the next global task as CTA-local task `gen`: one warp
-// (lane 0 takes the task, all lanes copy the pair's two FP32 rows).
-__device__ __forceinline__ void te_slot_fill(const TeBatch& B, long long total, TeSlot& S, float4* rows, int gen,
-                                             int lane)
+// (lane 0 takes the task, all lanes copy the pair's two FP32 rows through
+// put(T, frame e, a1's value, a2's value)).
+template <class Put>
+__device__ __forceinline__ void te_slot_fill_with(const TeBatch& B, long long total, TeSlot& S, int gen, int lane,
+                                                  Put put)
 {
     long long t = 0;
     int       d = 0;
@@ -857,10 +894,7 @@ __device__ __forceinline__ void te_slot_fill(const TeBatch& B, long long total, 
         const float4* x1 = p.X32 + (size_t)tk.a1 * T;
         const float4* x2 = p.X32 + (size_t)tk.a2 * T;
         for (int e = lane; e < T; e += 32)
-        {
-            rows[e]     = x1[e];
-            rows[T + e] = x2[e];
-        }
+            put(T, e, x1[e], x2[e]);
     }
     __syncwarp();
     if (lane == 0)
@@ -874,6 +908,26 @@ __device__ __forceinline__ void te_slot_fill(const TeBatch& B, long long total, 
         S.gen = gen;
     }
     __syncwarp();
+}
+
+__device__ __forceinline__ void te_slot_fill(const TeBatch& B, long long total, TeSlot& S, float4* rows, int gen,
+                                             int lane)
+{
+    te_slot_fill_with(B, total, S, gen, lane, [rows](int T, int e, const float4& a, const float4& b) {
+        rows[e]     = a;
+        rows[T + e] = b;
+    });
+}
+
+__device__ __forceinline__ void te_slot_fill12(const TeBatch& B, long long total, TeSlot& S, float2* xy, float* z,
+                                               int gen, int lane)
+{
+    te_slot_fill_with(B, total, S, gen, lane, [xy, z](int T, int e, const float4& a, const float4& b) {
+        xy[e]     = make_float2(a.x, a.y);
+        z[e]      = a.z;
+        xy[T + e] = make_float2(b.x, b.y);
+        z[T + e]  = b.z;
+    });
 }
 
 // The count kernel with two staged pair tasks per CTA (2 x 2 x maxT float4):
@@ -938,6 +992,68 @@ __global__ void __launch_bounds__(1024, 1) te_count_db_kernel(TeBatch B)
         last = __shfl_sync(kFull, last, 0);
         if (last) // every warp has left task i: its buffer takes task i + 2
             te_slot_fill(B, total, S, rows(b), i + 2, lane);
+    }
+}
+
+// The walk with two staged pair tasks per CTA (the count kernel's scheme):
+// per buffer the pair's rows as x,y float2 [2 maxT] and z float [2 maxT]
+// (24 maxT bytes), then each warp's histogram.
+template <bool LO>
+__global__ void __launch_bounds__(1024, 1) te_walk_db_kernel(TeBatch B)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ TeSlot slot[2];
+    const int         warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const long long   total = B.wprefix[B.n];
+    const int         maxT  = B.maxT;
+    auto              xyb   = [&](int b) { return reinterpret_cast<float2*>(smem_raw + (size_t)b * 24 * maxT); };
+    auto zb = [&](int b) { return reinterpret_cast<float*>(smem_raw + (size_t)b * 24 * maxT + (size_t)16 * maxT); };
+    unsigned char* base = smem_raw + (size_t)48 * maxT + (size_t)warp * kWalkBuckets * 32;
+    if (warp == 0)
+    {
+        te_slot_fill12(B, total, slot[0], xyb(0), zb(0), 0, lane);
+        te_slot_fill12(B, total, slot[1], xyb(1), zb(1), 1, lane);
+    }
+    __syncthreads();
+    for (int i = 0;; ++i)
+    {
+        const int b = i & 1;
+        TeSlot&   S = slot[b];
+        int       spins = 0;
+        while (S.gen != i)
+        {
+            if (++spins > (1 << 24))
+            {
+                if (lane == 0)
+                    atomicOr(B.d[0].status, kStatTimeout);
+                return;
+            }
+            __nanosleep(64);
+        }
+        __threadfence_block();
+        if (S.t < 0)
+            break;
+        const TeParams& p       = B.d[S.desc];
+        const TeTask    tk      = S.tk;
+        const int       ngroups = (p.Q + 31) >> 5;
+        const TeRows12  r1{xyb(b), zb(b)}, r2{xyb(b) + p.T, zb(b) + p.T};
+        for (;;)
+        {
+            int gi = 0;
+            if (lane == 0)
+                gi = atomicAdd(&S.next, 1);
+            gi          = __shfl_sync(kFull, gi, 0);
+            const int g = tk.c * B.chunk + gi;
+            if (gi >= B.chunk || g >= ngroups)
+                break;
+            te_walk_group<LO>(p, tk, g, r1, r2, base, lane);
+        }
+        int last = 0;
+        if (lane == 0)
+            last = atomicAdd(&S.left, 1) == nwarps - 1;
+        last = __shfl_sync(kFull, last, 0);
+        if (last)
+            te_slot_fill12(B, total, S, xyb(b), zb(b), i + 2, lane);
     }
 }
 
@@ -1068,9 +1184,14 @@ cudaError_t launch_te_rows(const TeBatch& b, long long rows, cudaStream_t s)
 cudaError_t launch_te_walk(const TeBatch& b, int warps, bool staged, int sms, cudaStream_t s)
 {
     const bool lo = b.maxK < 256;
-    void (*kernel)(TeBatch) = staged ? (lo ? te_walk_kernel<true, true> : te_walk_kernel<true, false>)
-                                     : (lo ? te_walk_kernel<false, true> : te_walk_kernel<false, false>);
-    const size_t smem = (staged ? (size_t)2 * b.maxT * 16 : 0) + (size_t)warps * kWalkBuckets * 32;
+    // two staged pair tasks per CTA (12-byte rows) where they fit beside the
+    // warps' histograms, else one (16-byte rows)
+    const size_t hist = (size_t)warps * kWalkBuckets * 32;
+    const bool   dbuf = staged && (size_t)48 * b.maxT + hist <= (size_t)226 * 1024;
+    void (*kernel)(TeBatch) = dbuf     ? (lo ? te_walk_db_kernel<true> : te_walk_db_kernel<false>)
+                              : staged ? (lo ? te_walk_kernel<true, true> : te_walk_kernel<true, false>)
+                                       : (lo ? te_walk_kernel<false, true> : te_walk_kernel<false, false>);
+    const size_t smem = (dbuf ? (size_t)48 * b.maxT : (staged ? (size_t)2 * b.maxT * 16 : 0)) + hist;
     cudaError_t  e    = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;

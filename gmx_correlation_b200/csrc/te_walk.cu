@@ -495,7 +495,7 @@ struct TeQuery64
 
 } // namespace
 
-__global__ void __launch_bounds__(kFinishWarps * 32, 1) te_finish_kernel(TeBatch B)
+__global__ void __launch_bounds__(kTeFinishWarps * 32, 1) te_finish_kernel(TeBatch B)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int      warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1206,16 +1206,16 @@ cudaError_t launch_te_walk(const TeBatch& b, int warps, bool staged, int sms, cu
 
 cudaError_t launch_te_finish(const TeBatch& b, int sms, cudaStream_t s)
 {
-    const size_t smem = (size_t)kFinishWarps * 6 * kTeBandCap * 32;
+    const size_t smem = (size_t)kTeFinishWarps * 6 * kTeBandCap * 32;
     cudaError_t  e    = cudaFuncSetAttribute(te_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, te_finish_kernel, kFinishWarps * 32, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, te_finish_kernel, kTeFinishWarps * 32, smem);
     if (e != cudaSuccess)
         return e;
     per_sm = per_sm < 1 ? 1 : per_sm;
-    te_finish_kernel<<<sms * per_sm, kFinishWarps * 32, smem, s>>>(b);
+    te_finish_kernel<<<sms * per_sm, kTeFinishWarps * 32, smem, s>>>(b);
     return cudaGetLastError();
 }
 

@@ -19,6 +19,10 @@
 namespace gc {
 
 constexpr int kTeBandCap = 24; // band entries kept per lane in the finish kernel
+#ifndef GC_TE_FINISH_WARPS
+#define GC_TE_FINISH_WARPS 24 // a build-time setting for timing other finish CTA shapes
+#endif
+constexpr int kTeFinishWarps = GC_TE_FINISH_WARPS; // warps per TE finish CTA
 
 // One query block of one trajectory.  Entry m of the G row of (atom a,
 // query i0 + iq) is element ((a * Lq + m / 4) * Qp + iq) * 4 + m % 4 of

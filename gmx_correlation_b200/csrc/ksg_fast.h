@@ -7,7 +7,10 @@
 namespace gc {
 
 constexpr int kWalkWarps   = 32;       // most warps per walk CTA
-constexpr int kFinishWarps = 16;       // warps per finish CTA
+#ifndef GC_FINISH_WARPS
+#define GC_FINISH_WARPS 16 // a build-time setting for timing other finish CTA shapes
+#endif
+constexpr int kFinishWarps = GC_FINISH_WARPS; // warps per finish CTA
 constexpr int kWalkBuckets = 128;      // per-lane histogram buckets
 #ifndef GC_BAND_CAP
 #define GC_BAND_CAP 20 // a build-time setting for timing other capacities

@@ -774,21 +774,22 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
                     nlo += v < elo;
                 };
                 // Both ranges by aligned 4-entry groups of the row (one 16-byte
-                // and one 8-byte load per group), two groups per round, so the
-                // loads of a round and then its gathers overlap.
-                for (int g0 = mw0 >> 2; g0 * 4 < mw1; g0 += 2) // s in the band, d <= bandhi
+                // and one 8-byte load per group), kFinishRound groups per round
+                // (the loads of a round, then its gathers).  One group per round
+                // keeps the kernel at 96 registers, so a CTA holds 20 warps.
+                for (int g0 = mw0 >> 2; g0 * 4 < mw1; g0 += kFinishRound) // s in the band, d <= bandhi
                 {
-                    float4 s4[2];
-                    uint2  j4[2];
+                    float4 s4[kFinishRound];
+                    uint2  j4[kFinishRound];
 #pragma unroll
-                    for (int h = 0; h < 2; ++h)
+                    for (int h = 0; h < kFinishRound; ++h)
                         if ((g0 + h) * 4 < mw1)
                         {
                             s4[h] = rw.s4(g0 + h);
                             j4[h] = rw.j4(g0 + h);
                         }
 #pragma unroll
-                    for (int h = 0; h < 2; ++h)
+                    for (int h = 0; h < kFinishRound; ++h)
 #pragma unroll
                         for (int q = 0; q < 4; ++q)
                         {
@@ -802,19 +803,19 @@ __global__ void __launch_bounds__(kFinishWarps * 32, 1) ksg_finish_kernel(WalkBa
                         }
                 }
                 const int nW = nband; // band entries from the walked row come first
-                for (int g0 = mo0 >> 2; g0 * 4 < mo1; g0 += 2) // d in the band, s < inlo
+                for (int g0 = mo0 >> 2; g0 * 4 < mo1; g0 += kFinishRound) // d in the band, s < inlo
                 {
-                    float4 d4[2];
-                    uint2  j4[2];
+                    float4 d4[kFinishRound];
+                    uint2  j4[kFinishRound];
 #pragma unroll
-                    for (int h = 0; h < 2; ++h)
+                    for (int h = 0; h < kFinishRound; ++h)
                         if ((g0 + h) * 4 < mo1)
                         {
                             d4[h] = ro.s4(g0 + h);
                             j4[h] = ro.j4(g0 + h);
                         }
 #pragma unroll
-                    for (int h = 0; h < 2; ++h)
+                    for (int h = 0; h < kFinishRound; ++h)
 #pragma unroll
                         for (int q = 0; q < 4; ++q)
                         {

@@ -8,9 +8,13 @@ namespace gc {
 
 constexpr int kWalkWarps   = 32;       // most warps per walk CTA
 #ifndef GC_FINISH_WARPS
-#define GC_FINISH_WARPS 16 // a build-time setting for timing other finish CTA shapes
+#define GC_FINISH_WARPS 20 // a build-time setting for timing other finish CTA shapes
 #endif
 constexpr int kFinishWarps = GC_FINISH_WARPS; // warps per finish CTA
+#ifndef GC_FINISH_ROUND
+#define GC_FINISH_ROUND 1 // a build-time setting: 4-entry row groups loaded per band round
+#endif
+constexpr int kFinishRound = GC_FINISH_ROUND;
 constexpr int kWalkBuckets = 128;      // per-lane histogram buckets
 #ifndef GC_BAND_CAP
 #define GC_BAND_CAP 20 // a build-time setting for timing other capacities

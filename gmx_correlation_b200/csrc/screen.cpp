@@ -247,14 +247,18 @@ gc_status list_to_ab(const int64_t* list, long n, long npairs, std::vector<int2>
 gc_status features_device(const double* d_xyz, int natoms, int T, int k, long pair_begin, long count,
                           const int2* d_ab, const float* d_pca, float* d_out, cudaStream_t s)
 {
-    DevBuf<double>        stats;
-    DevBuf<unsigned char> bins;
+    // pooled scratch (no cudaMalloc / cudaFree per call); the stream is
+    // synchronised before the blocks return to the pool
+    PoolBuf<double>        stats;
+    PoolBuf<unsigned char> bins;
     GC_TRY(stats.alloc((size_t)natoms * gc::kScreenStat));
     GC_TRY(bins.alloc((size_t)natoms * T));
-    const int width = d_pca ? gc::kScreenIn : gc::kScreenBase + gc::kScreenHist;
-    GC_TRY_CUDA(gc::launch_screen_features(d_xyz, natoms, T, k, pair_begin, count, d_ab, d_pca, gc::kScreenComp,
-                                           stats.p, bins.p, d_out, width, s));
-    GC_TRY_CUDA(cudaStreamSynchronize(s));
+    const int         width = d_pca ? gc::kScreenIn : gc::kScreenBase + gc::kScreenHist;
+    const cudaError_t e     = gc::launch_screen_features(d_xyz, natoms, T, k, pair_begin, count, d_ab, d_pca,
+                                                         gc::kScreenComp, stats.p, bins.p, d_out, width, s);
+    const cudaError_t w     = cudaStreamSynchronize(s);
+    GC_TRY_CUDA(e);
+    GC_TRY_CUDA(w);
     return GC_OK;
 }
 

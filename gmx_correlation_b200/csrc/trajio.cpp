@@ -77,6 +77,17 @@ struct XdrIn
 {
     FILE* f;
 
+    // bytes from the read position to the end of the file
+    long left() const
+    {
+        const long here = std::ftell(f);
+        if (here < 0 || std::fseek(f, 0, SEEK_END) != 0)
+            return 0;
+        const long end = std::ftell(f);
+        std::fseek(f, here, SEEK_SET);
+        return end > here ? end - here : 0;
+    }
+
     bool raw(void* p, size_t n) { return std::fread(p, 1, n, f) == n; }
     bool u32(uint32_t& v)
     {
@@ -388,9 +399,9 @@ bool xtc_coords(XdrIn& in, int natoms, std::vector<float>& x, std::vector<unsign
         return bad("truncated XTC frame");
     if (lsize != natoms)
         return bad("XTC frame: atom counts of header and coordinates differ");
-    x.resize((size_t)natoms * 3);
     if (natoms <= 9)
     {
+        x.resize((size_t)natoms * 3);
         for (int i = 0; i < natoms * 3; ++i)
             if (!in.f32(x[(size_t)i]))
                 return bad("truncated XTC frame");
@@ -403,6 +414,10 @@ bool xtc_coords(XdrIn& in, int natoms, std::vector<float>& x, std::vector<unsign
         return bad("truncated XTC frame");
     if (!(precision > 0.0f) || smallidx < kFirstIdx || smallidx >= kLastIdx || nbytes < 0)
         return bad("corrupt XTC frame header");
+    // every atom takes at least one bit of the stream, which the file holds
+    if ((long long)natoms > 8LL * nbytes + 8 || (long long)nbytes > in.left())
+        return bad("corrupt XTC frame: more atoms or bytes than the file holds");
+    x.resize((size_t)natoms * 3);
     unsigned sizeint[3];
     int      bitsizeint[3] = {0, 0, 0}, bitsize = 0;
     bool     large = false;
@@ -741,6 +756,8 @@ bool trr_frame(XdrIn& in, Frame& fr, bool keep_double)
         return bad("corrupt TRR header: block sizes disagree with the atom count");
     if (!xs)
         return bad("TRR frame without positions");
+    if ((long long)box + vir + pres + xs + vs + fs > in.left())
+        return bad("truncated TRR frame");
     if (!in.skip((long)box + vir + pres))
         return bad("truncated TRR frame");
     fr.natoms = natoms;
@@ -837,9 +854,32 @@ gc_status each_frame(const char* path, bool keep_double, int* format, Fn fn)
 
 } // namespace
 
+namespace {
+
+// The entry points: no C++ exception crosses the C ABI (a file announcing an
+// absurd atom count could otherwise end the process with std::bad_alloc).
+template <class F>
+gc_status guarded(const char* what, F&& f)
+{
+    try
+    {
+        return f();
+    }
+    catch (const std::bad_alloc&)
+    {
+        return fail(GC_ERR_OUT_OF_MEMORY, std::string(what) + ": host allocation failed (a corrupt atom count?)");
+    }
+    catch (const std::exception& e)
+    {
+        return fail(GC_ERR_INTERNAL, std::string(what) + ": " + e.what());
+    }
+}
+
+} // namespace
+
 extern "C" {
 
-gc_status gc_traj_info(const char* path, int* format, int* natoms, int* nframes)
+static gc_status traj_info_impl(const char* path, int* format, int* natoms, int* nframes)
 {
     if (!path)
         return fail(GC_ERR_INVALID, "gc_traj_info: null path");
@@ -863,7 +903,8 @@ gc_status gc_traj_info(const char* path, int* format, int* natoms, int* nframes)
     return GC_OK;
 }
 
-gc_status gc_traj_read(const char* path, const gc_traj_select* sel, double** xyz, int* natoms, int* nframes)
+static gc_status traj_read_impl(const char* path, const gc_traj_select* sel, double** xyz, int* natoms,
+                                int* nframes)
 {
     if (!path || !xyz || !natoms || !nframes)
         return fail(GC_ERR_INVALID, "gc_traj_read: null argument");
@@ -948,7 +989,8 @@ gc_status gc_traj_read(const char* path, const gc_traj_select* sel, double** xyz
 
 void gc_traj_free(double* xyz) { std::free(xyz); }
 
-gc_status gc_traj_write(const char* path, int format, const float* xyz, int natoms, int nframes, const float* box,
+static gc_status traj_write_impl(const char* path, int format, const float* xyz, int natoms, int nframes,
+                                 const float* box,
                         const double* times, float precision, int flags)
 {
     if (!path || !xyz || natoms < 1 || nframes < 0)
@@ -1015,6 +1057,25 @@ gc_status gc_traj_write(const char* path, int format, const float* xyz, int nato
             return fail(GC_ERR_IO, std::string("write error on ") + path);
     }
     return GC_OK;
+}
+
+// The guarded entry points follow.
+
+gc_status gc_traj_info(const char* path, int* format, int* natoms, int* nframes)
+{
+    return guarded("gc_traj_info", [&] { return traj_info_impl(path, format, natoms, nframes); });
+}
+
+gc_status gc_traj_read(const char* path, const gc_traj_select* sel, double** xyz, int* natoms, int* nframes)
+{
+    return guarded("gc_traj_read", [&] { return traj_read_impl(path, sel, xyz, natoms, nframes); });
+}
+
+gc_status gc_traj_write(const char* path, int format, const float* xyz, int natoms, int nframes, const float* box,
+                        const double* times, float precision, int flags)
+{
+    return guarded("gc_traj_write",
+                   [&] { return traj_write_impl(path, format, xyz, natoms, nframes, box, times, precision, flags); });
 }
 
 } // extern "C"

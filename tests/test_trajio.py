@@ -300,3 +300,21 @@ def test_cli_selection_errors(tmp_path):
     assert r.returncode != 0 and "outside" in r.stderr
     r = _cli("-f", p, "-sel", "x")
     assert r.returncode != 0 and "neither an index group" in r.stderr
+
+
+def test_absurd_atom_counts_fail_without_allocating(tmp_path, gc):
+    # a corrupt header announcing a billion atoms is rejected from the bytes
+    # the file holds, before anything is allocated for them
+    n = 1 << 30
+    head = struct.pack(">iiif", 1995, n, 0, 0.0) + struct.pack(">9f", *np.eye(3).ravel()) + struct.pack(">i", n)
+    body = struct.pack(">f6iii", 1000.0, 0, 0, 0, 1, 1, 1, 9, 8) + bytes(8)
+    p = tmp_path / "huge.xtc"
+    p.write_bytes(head + body)
+    with pytest.raises(gc.GCError, match="more atoms or bytes"):
+        trajio.read_trajectory(p)
+    t = tmp_path / "huge.trr"
+    t.write_bytes(struct.pack(">iii", 1993, 13, 12) + b"GMX_trn_file" +
+                  struct.pack(">11i", 0, 0, 0, 0, 0, 0, 0, (1 << 26) * 12, 0, 0, 1 << 26) +
+                  struct.pack(">iiff", 0, 0, 0.0, 0.0) + bytes(64))
+    with pytest.raises(gc.GCError, match="truncated"):
+        trajio.read_trajectory(t)

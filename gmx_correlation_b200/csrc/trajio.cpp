@@ -122,6 +122,25 @@ struct XdrIn
         std::memcpy(&v, &u, 8);
         return true;
     }
+    // n big-endian 4-byte floats / 8-byte doubles in one read
+    bool f32s(float* v, size_t n)
+    {
+        if (!raw(v, n * 4))
+            return false;
+        uint32_t* u = reinterpret_cast<uint32_t*>(v);
+        for (size_t i = 0; i < n; ++i)
+            u[i] = __builtin_bswap32(u[i]);
+        return true;
+    }
+    bool f64s(double* v, size_t n)
+    {
+        if (!raw(v, n * 8))
+            return false;
+        uint64_t* u = reinterpret_cast<uint64_t*>(v);
+        for (size_t i = 0; i < n; ++i)
+            u[i] = __builtin_bswap64(u[i]);
+        return true;
+    }
     // n bytes of opaque data and the padding to a multiple of 4
     bool opaque(unsigned char* p, size_t n)
     {
@@ -253,61 +272,55 @@ struct BitIn
 {
     const unsigned char* p;
     size_t               n, pos = 0; // bytes, next byte
-    uint32_t             acc = 0;   // bits not consumed yet, right-aligned
-    int                  have = 0;  // how many
+    uint64_t             acc  = 0;   // bits not consumed yet are the low `have` bits
+    int                  have = 0;
     bool                 over = false;
 
+    // the next nbits (0 .. 32) bits as an unsigned integer
     uint32_t get(int nbits)
     {
-        uint32_t v = 0;
-        while (nbits > 0)
+        while (have < nbits)
         {
-            if (have == 0)
+            if (pos >= n)
             {
-                if (pos >= n)
-                {
-                    over = true;
-                    return 0;
-                }
-                acc  = p[pos++];
-                have = 8;
+                over = true;
+                return 0;
             }
-            const int take = std::min(nbits, have);
-            v              = (v << take) | ((acc >> (have - take)) & ((1u << take) - 1));
-            have -= take;
-            nbits -= take;
+            acc = (acc << 8) | p[pos++];
+            have += 8;
         }
-        return v;
+        have -= nbits;
+        return (uint32_t)((acc >> have) & ((1ull << nbits) - 1ull));
     }
-    // Three integers of a mixed-radix number of nbits bits (little-endian
-    // bytes, first byte first, the last one holding the remaining bits).
+    // Three integers of a mixed-radix number of nbits bits: its bytes come
+    // least significant first (the last one holds the remaining bits), the
+    // number is ((v0 * s1) + v1) * s2 + v2.
     void get3(int nbits, const unsigned sizes[3], int out[3])
     {
-        unsigned char bytes[32];
-        int           nb = 0;
-        while (nbits > 8 && nb < 31)
+        if (nbits <= 64)
         {
-            bytes[nb++] = (unsigned char)get(8);
-            nbits -= 8;
+            uint64_t num = 0;
+            int      sh = 0, rem = nbits;
+            for (; rem > 8; rem -= 8, sh += 8)
+                num |= (uint64_t)get(8) << sh;
+            if (rem > 0)
+                num |= (uint64_t)get(rem) << sh;
+            out[2] = (int)(num % sizes[2]);
+            num /= sizes[2];
+            out[1] = (int)(num % sizes[1]);
+            out[0] = (int)(uint32_t)(num / sizes[1]);
+            return;
         }
-        if (nbits > 0)
-            bytes[nb++] = (unsigned char)get(nbits);
-        for (int i = 2; i > 0; --i)
-        {
-            uint64_t rem = 0;
-            for (int j = nb - 1; j >= 0; --j)
-            {
-                rem            = (rem << 8) | bytes[j];
-                const uint64_t q = rem / sizes[i];
-                bytes[j]       = (unsigned char)q;
-                rem -= q * sizes[i];
-            }
-            out[i] = (int)rem;
-        }
-        uint32_t v = 0;
-        for (int j = std::min(nb, 4) - 1; j >= 0; --j)
-            v = (v << 8) | bytes[j];
-        out[0] = (int)v;
+        unsigned __int128 num = 0;
+        int               sh = 0, rem = nbits;
+        for (; rem > 8; rem -= 8, sh += 8)
+            num |= (unsigned __int128)get(8) << sh;
+        if (rem > 0)
+            num |= (unsigned __int128)get(rem) << sh;
+        out[2] = (int)(uint64_t)(num % sizes[2]);
+        num /= sizes[2];
+        out[1] = (int)(uint64_t)(num % sizes[1]);
+        out[0] = (int)(uint32_t)(uint64_t)(num / sizes[1]);
     }
 };
 
@@ -768,17 +781,15 @@ bool trr_frame(XdrIn& in, Frame& fr, bool keep_double)
     if (real == 4)
     {
         fr.xf.resize((size_t)per);
-        for (float& v : fr.xf)
-            if (!in.f32(v))
-                return bad("truncated TRR frame");
+        if (!in.f32s(fr.xf.data(), (size_t)per))
+            return bad("truncated TRR frame");
     }
     else
     {
         std::vector<double>& dst = fr.xd;
         dst.resize((size_t)per);
-        for (double& v : dst)
-            if (!in.f64(v))
-                return bad("truncated TRR frame");
+        if (!in.f64s(dst.data(), (size_t)per))
+            return bad("truncated TRR frame");
         if (!keep_double)
         {
             fr.xf.assign(dst.begin(), dst.end()); // rounded to float, as a mixed-precision reader does
@@ -917,7 +928,9 @@ static gc_status traj_read_impl(const char* path, const gc_traj_select* sel, dou
         return fail(GC_ERR_INVALID, "The -skip value must be at least 1.");
     if (s.natoms < 0 || (s.natoms > 0 && !s.atoms))
         return fail(GC_ERR_INVALID, "gc_traj_read: selection without atom indices");
-    std::vector<double> frames; // kept frames, frame-major, selected atoms
+    // kept frames, one block of the selected atoms' positions each (no
+    // reallocation of one growing buffer)
+    std::vector<std::unique_ptr<double[]>> frames;
     int                 nsel = -1, file_atoms = -1;
     long long           analysed = 0; // frames inside the time window, as the reference counts frnr
     gc_status           st       = GC_OK;
@@ -946,40 +959,50 @@ static gc_status traj_read_impl(const char* path, const gc_traj_select* sel, dou
         if (analysed++ % s.skip != 0)
             return true;
         const bool dbl = !fr.xd.empty();
+        frames.emplace_back(new double[(size_t)nsel * 3]);
+        double* out = frames.back().get();
         for (int i = 0; i < nsel; ++i)
         {
             const size_t a = (size_t)(s.natoms > 0 ? s.atoms[i] : i) * 3;
             for (int d = 0; d < 3; ++d)
-                frames.push_back(dbl ? fr.xd[a + d] : (double)fr.xf[a + d]);
+                out[(size_t)i * 3 + d] = dbl ? fr.xd[a + d] : (double)fr.xf[a + d];
         }
         return true;
     }));
     GC_TRY(st);
-    const size_t T = nsel > 0 ? frames.size() / ((size_t)nsel * 3) : 0;
+    const size_t T = nsel > 0 ? frames.size() : 0;
     if (T == 0)
         return fail(GC_ERR_INVALID, "No trajectory frames were selected for analysis.");
     if (T > (size_t)gc::kMaxFrames)
         return fail(GC_ERR_INVALID, "gc_traj_read: more frames than the library handles");
-    double* out = static_cast<double*>(std::malloc(sizeof(double) * frames.size()));
+    double* out = static_cast<double*>(std::malloc(sizeof(double) * T * (size_t)nsel * 3));
     if (!out)
         return fail(GC_ERR_OUT_OF_MEMORY, "gc_traj_read: host allocation failed");
     // x[atom][frame][dim]; with GC_TRAJ_CENTER each atom's mean position
     // (summed in frame order, then divided) is subtracted, as the reference
     // module does before the estimators run
-    for (int a = 0; a < nsel; ++a)
+    // every atom's sum still runs over its frames in order; the passes go
+    // frame by frame, the transpose in tiles of frames
+    std::vector<double> av((size_t)nsel * 3, 0.0);
+    if (s.flags & GC_TRAJ_CENTER)
     {
-        double av[3] = {0.0, 0.0, 0.0};
-        if (s.flags & GC_TRAJ_CENTER)
-        {
-            for (size_t t = 0; t < T; ++t)
-                for (int d = 0; d < 3; ++d)
-                    av[d] += frames[(t * nsel + a) * 3 + d];
-            for (int d = 0; d < 3; ++d)
-                av[d] /= (double)T;
-        }
         for (size_t t = 0; t < T; ++t)
-            for (int d = 0; d < 3; ++d)
-                out[((size_t)a * T + t) * 3 + d] = frames[(t * nsel + a) * 3 + d] - av[d];
+        {
+            const double* f = frames[t].get();
+            for (size_t e = 0; e < (size_t)nsel * 3; ++e)
+                av[e] += f[e];
+        }
+        for (double& v : av)
+            v /= (double)T;
+    }
+    constexpr size_t kTile = 32;
+    for (size_t t0 = 0; t0 < T; t0 += kTile)
+    {
+        const size_t t1 = std::min(T, t0 + kTile);
+        for (int a = 0; a < nsel; ++a)
+            for (size_t t = t0; t < t1; ++t)
+                for (int d = 0; d < 3; ++d)
+                    out[((size_t)a * T + t) * 3 + d] = frames[t][(size_t)a * 3 + d] - av[(size_t)a * 3 + d];
     }
     *xyz     = out;
     *natoms  = nsel;

@@ -73,3 +73,49 @@ def test_cpp_dropin_links_every_reference_symbol(gc, tmp_path):
                           str(ROOT / "tests" / "dropin_check.cpp"), "-o", str(tmp_path / "dropin_check"),
                           f"-L{pkg}", "-lgmxcorr_b200", "-Wl,--no-undefined"], capture_output=True, text=True)
     assert res.returncode == 0, res.stderr
+
+
+def test_cpp_dropin_links_every_milca_function(gc, tmp_path):
+    """Code written against the MILCA definitions of lib/kraskov.cpp
+    (:347-2155, no header in the reference) links against the library through
+    csrc/dropin/kraskov_milca.h with the same signatures (nothing runs here)."""
+    import shutil
+    import subprocess
+    src = tmp_path / "milca_check.cpp"
+    src.write_text(r'''
+#include "kraskov_milca.h"
+int main(int argc, char**)
+{
+    if (argc > 1) // never taken: only the symbols must resolve
+    {
+        double *x[4] = {}, psi[8] = {}, scal[4] = {}, a = 0, b = 0, c = 0, d = 0, cr[8] = {};
+        float  f[8] = {};
+        int    *ip = nullptr, **ipp = nullptr;
+        double **dpp = nullptr;
+        mi2(x, 8, 1, psi, scal, &a, &b);
+        mi2c(x, 8, 1, psi, scal, &a);
+        mi2r(x, 8, 1, psi, scal, &b);
+        mi2r_(x, 8, 1, psi, scal, &b);
+        mi2K(x, 8, 1, psi, scal, cr);
+        mi2h(x, 8, 1, psi, scal, &a, &b, &c, &d);
+        red(x, 2, 8, 1, psi, scal, &a, &b);
+        redc(x, 2, 8, 1, psi, scal, &a);
+        redr(x, 2, 8, 1, psi, scal, &b);
+        redK(x, 2, 8, 1, psi, scal, cr);
+        redr_embed(x, 2, 2, 1, 8, 1, psi, &b);
+        mi_xnyn(x, 1, 1, 8, 1, psi, scal, &a, &b);
+        mic_xnyn(x, 1, 1, 8, 1, psi, scal, &a);
+        mir_xnyn(x, 1, 1, 8, 1, psi, scal, &b);
+        mi_xnynK(x, 1, 1, 8, 1, psi, scal, cr);
+        mi_xnynKembed(x, 1, 8, 1, dpp, dpp, ipp, ip, ip, ipp, ip, ip, psi, cr);
+        mi_d(x, 2, 8, 1, f, psi, psi, 0.0, 1.0, 0.0, 1.0);
+    }
+    return 0;
+}
+''')
+    cxx = "/usr/bin/g++" if shutil.which("/usr/bin/g++") else "g++"
+    pkg = ROOT / "gmx_correlation_b200"
+    res = subprocess.run([cxx, "-O0", "-std=c++17", f"-I{pkg / 'csrc' / 'dropin'}", str(src),
+                          "-o", str(tmp_path / "milca_check"), f"-L{pkg}", "-lgmxcorr_b200", "-Wl,--no-undefined"],
+                         capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr

@@ -153,8 +153,9 @@ gc_status gc_gauss_matrix(const gc_traj_view* traj, const gc_opts* opts, double*
  * graph; the workspace and graph of the last batch (shapes and lag) are
  * kept for a repeated call (gc_te_batch_release frees them; the per-query
  * counts take 8 bytes per ordered pair and frame, about 22 GB for 16
- * trajectories of up to 400 atoms x 4000 frames, beside up to 24 GiB of
- * sorted rows).  No counterpart in the reference, which computes te_matrix
+ * trajectories of up to 400 atoms x 4000 frames, beside one arena of
+ * sorted rows shared by all waves: 32 GiB, or one trajectory's largest query
+ * block of at most 16 GiB where that is larger).  No counterpart in the reference, which computes te_matrix
  * per trajectory.  opts: device only. */
 gc_status gc_te_batch(const gc_traj_view* trajs, const int* ks, int ntraj, int lag, const gc_opts* opts,
                       double* const* te);

@@ -131,19 +131,30 @@ gc_status run(Call& c)
 
     DeviceScope dev(-1);
     GC_TRY(dev.st);
+    // the call's own stream; pooled buffers, returned only after the stream
+    // has drained (the guard is destroyed before them, on every path)
+    StreamScope ss;
+    GC_TRY(ss.init(nullptr));
+    const cudaStream_t st = ss.s;
     const int          Kr = c.krange ? c.K : 1;
     const size_t       nq = (size_t)c.N * Kr;
-    DevBuf<double>     X, psi, phi, eps, mic, mir;
-    DevBuf<int>        cnt, maxd, order, status;
+    PoolBuf<double>    X, psi, phi, eps, mic, mir;
+    PoolBuf<int>       cnt, maxd, order, status;
+    struct Drain
+    {
+        cudaStream_t s;
+        ~Drain() { cudaStreamSynchronize(s); }
+    } drain{st};
     GC_TRY(X.alloc((size_t)D * c.N));
     for (int d = 0; d < D; ++d)
-        GC_TRY_CUDA(cudaMemcpy(X.p + (size_t)d * c.N, c.rows[(size_t)d], sizeof(double) * c.N, cudaMemcpyHostToDevice));
+        GC_TRY_CUDA(cudaMemcpyAsync(X.p + (size_t)d * c.N, c.rows[(size_t)d], sizeof(double) * c.N,
+                                    cudaMemcpyHostToDevice, st));
     GC_TRY(psi.alloc((size_t)c.N + 1));
-    GC_TRY_CUDA(cudaMemcpy(psi.p, c.psi, sizeof(double) * (c.N + 1), cudaMemcpyHostToDevice));
+    GC_TRY_CUDA(cudaMemcpyAsync(psi.p, c.psi, sizeof(double) * (c.N + 1), cudaMemcpyHostToDevice, st));
     if (c.phi)
     {
         GC_TRY(phi.alloc((size_t)c.K + 1));
-        GC_TRY_CUDA(cudaMemcpy(phi.p, c.phi, sizeof(double) * (c.K + 1), cudaMemcpyHostToDevice));
+        GC_TRY_CUDA(cudaMemcpyAsync(phi.p, c.phi, sizeof(double) * (c.K + 1), cudaMemcpyHostToDevice, st));
     }
     GC_TRY(eps.alloc(nq * (G + 1)));
     GC_TRY(cnt.alloc(nq * G * 2));
@@ -158,8 +169,8 @@ gc_status run(Call& c)
         for (int i = 0; i < c.N; ++i)
             c.order[(size_t)i] = i;
     GC_TRY(order.alloc((size_t)c.N));
-    GC_TRY_CUDA(cudaMemcpy(order.p, c.order.data(), sizeof(int) * c.N, cudaMemcpyHostToDevice));
-    GC_TRY_CUDA(cudaMemset(status.p, 0, sizeof(int)));
+    GC_TRY_CUDA(cudaMemcpyAsync(order.p, c.order.data(), sizeof(int) * c.N, cudaMemcpyHostToDevice, st));
+    GC_TRY_CUDA(cudaMemsetAsync(status.p, 0, sizeof(int), st));
 
     gc::MilcaParams p{};
     p.X = X.p;
@@ -196,24 +207,25 @@ gc_status run(Call& c)
     s.pair_sum = c.pair_sum;
     s.mic      = mic.p;
     s.mir      = mir.p;
-    GC_TRY_CUDA(gc::launch_milca(p, s, nullptr));
-    GC_TRY_CUDA(cudaDeviceSynchronize());
-    int st = 0;
-    GC_TRY_CUDA(cudaMemcpy(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost));
-    GC_TRY(status_to_error(st));
+    GC_TRY_CUDA(gc::launch_milca(p, s, st));
+    int stw = 0;
+    GC_TRY_CUDA(cudaMemcpyAsync(&stw, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    GC_TRY_CUDA(cudaStreamSynchronize(st));
+    GC_TRY(status_to_error(stw));
     c.mic.resize((size_t)Kr);
     c.mir.resize((size_t)Kr);
-    GC_TRY_CUDA(cudaMemcpy(c.mic.data(), mic.p, sizeof(double) * Kr, cudaMemcpyDeviceToHost));
-    GC_TRY_CUDA(cudaMemcpy(c.mir.data(), mir.p, sizeof(double) * Kr, cudaMemcpyDeviceToHost));
+    GC_TRY_CUDA(cudaMemcpyAsync(c.mic.data(), mic.p, sizeof(double) * Kr, cudaMemcpyDeviceToHost, st));
+    GC_TRY_CUDA(cudaMemcpyAsync(c.mir.data(), mir.p, sizeof(double) * Kr, cudaMemcpyDeviceToHost, st));
     if (c.want_detail)
     {
         c.eps.resize(nq * (G + 1));
         c.cnt.resize(nq * G * 2);
         c.maxd.resize(nq);
-        GC_TRY_CUDA(cudaMemcpy(c.eps.data(), eps.p, sizeof(double) * c.eps.size(), cudaMemcpyDeviceToHost));
-        GC_TRY_CUDA(cudaMemcpy(c.cnt.data(), cnt.p, sizeof(int) * c.cnt.size(), cudaMemcpyDeviceToHost));
-        GC_TRY_CUDA(cudaMemcpy(c.maxd.data(), maxd.p, sizeof(int) * c.maxd.size(), cudaMemcpyDeviceToHost));
+        GC_TRY_CUDA(cudaMemcpyAsync(c.eps.data(), eps.p, sizeof(double) * c.eps.size(), cudaMemcpyDeviceToHost, st));
+        GC_TRY_CUDA(cudaMemcpyAsync(c.cnt.data(), cnt.p, sizeof(int) * c.cnt.size(), cudaMemcpyDeviceToHost, st));
+        GC_TRY_CUDA(cudaMemcpyAsync(c.maxd.data(), maxd.p, sizeof(int) * c.maxd.size(), cudaMemcpyDeviceToHost, st));
     }
+    GC_TRY_CUDA(cudaStreamSynchronize(st));
     return GC_OK;
 }
 
